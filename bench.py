@@ -1,0 +1,410 @@
+"""Benchmark of the MKF hot path on B200: scalar field -> K binary pattern distributions.
+
+Workload (N=1): a 1024^3 FP64 Gaussian random field (N(0,1) white noise from a fixed seed,
+periodic Gaussian smoothing sigma = 4 voxels, renormalised to zero mean / unit variance) with 16
+thresholds evenly spaced in [-2, 2], relation '>'. One step = one read of the field giving 16
+distributions (mkfFieldBPFD) plus their Minkowski measures on the device (mkfMeasuresF64Dev).
+Inputs are 8.6 GB, far larger than the 126 MB L2, so no flush is needed between steps.
+
+  value     Gvoxel/s with the field resident in HBM (device-timed, max over ranks)
+  e2e       Gvoxel/s through the host-buffer entry point mkfFieldBPFDHost: each step copies the
+            pinned host field to the GPU (slabs overlapped with counting) and the counts back
+  roofline  the fused kernel's algorithmic bytes / its CUDA-event time vs measured HBM peak
+  cpu_baseline  the reference MKF C path (compiled from its sources) on this host's cores, on a
+            bounded slab sample of the same kind of field
+
+With torchrun (N > 1) every rank counts its own 1024^3 slab (1025 planes: one halo plane) of a
+field sharded along z and the 16 x 256 partial counts are summed with an NCCL all-reduce each
+step (weak scaling). `--impl reference` times the reference C path alone (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+N_SIDE = 1024
+SIGMA = 4.0
+K_THRESH = 16
+THRESHOLDS = np.linspace(-2.0, 2.0, K_THRESH)
+SEED = 20261203
+WORKLOAD = "grf1024_f64_k16"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="mkf", choices=["mkf", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- synthetic fields
+
+def grf_torch(nz, ny, nx, seed, device):
+    """Gaussian random field on the GPU (FFT smoothing), FP64, zero mean, unit variance."""
+    import torch
+
+    g = torch.Generator(device=device).manual_seed(seed)
+    w = torch.randn((nz, ny, nx), dtype=torch.float64, device=device, generator=g)
+    W = torch.fft.rfftn(w)
+    del w
+    two_pi = 2 * math.pi
+    for dim, n in ((0, nz), (1, ny)):
+        k = torch.fft.fftfreq(n, device=device, dtype=torch.float64) * two_pi
+        shape = [1, 1, 1]
+        shape[dim] = n
+        W *= torch.exp(-0.5 * SIGMA * SIGMA * k * k).view(shape)
+    kx = torch.fft.rfftfreq(nx, device=device, dtype=torch.float64) * two_pi
+    W *= torch.exp(-0.5 * SIGMA * SIGMA * kx * kx).view(1, 1, -1)
+    f = torch.fft.irfftn(W, s=(nz, ny, nx))
+    del W
+    f -= f.mean()
+    f /= f.std()
+    torch.cuda.synchronize(device)
+    return f.contiguous()
+
+
+def grf_numpy(nz, ny, nx, seed):
+    """The same kind of field on the host (for the CPU runs), with 64 elements of slack after the
+    end because the reference CPU map reads past each row when X % 32 != 0."""
+    rng = np.random.default_rng(seed)
+    w = rng.standard_normal((nz, ny, nx))
+    W = np.fft.rfftn(w)
+    del w
+    two_pi = 2 * math.pi
+    kz = np.fft.fftfreq(nz) * two_pi
+    ky = np.fft.fftfreq(ny) * two_pi
+    kx = np.fft.rfftfreq(nx) * two_pi
+    W *= np.exp(-0.5 * SIGMA * SIGMA * kz * kz)[:, None, None]
+    W *= np.exp(-0.5 * SIGMA * SIGMA * ky * ky)[None, :, None]
+    W *= np.exp(-0.5 * SIGMA * SIGMA * kx * kx)[None, None, :]
+    f = np.fft.irfftn(W, s=(nz, ny, nx))
+    f -= f.mean()
+    f /= f.std()
+    flat = np.zeros(f.size + 64, np.float64)
+    flat[: f.size] = f.ravel()
+    return flat
+
+
+# ---------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 50 ms in the background."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.rows = []
+        self.proc = None
+        self.gpu_id = gpu_id
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.gpu_id, "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+
+        def reader():
+            for line in self.proc.stdout:
+                self.rows.append((time.time(), [c.strip() for c in line.split(",")]))
+
+        self.thread = threading.Thread(target=reader, daemon=True)
+        self.thread.start()
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+
+    def summary(self, t0, t1):
+        rows = [r for ts, r in self.rows if t0 <= ts <= t1 and len(r) >= 9]
+        if not rows:
+            after = [r for ts, r in self.rows if ts >= t0 and len(r) >= 9]
+            rows = after[:3]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        mx = [num(r[2]) for r in rows if num(r[2]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def gpu_id_of(dev_index: int) -> str:
+    import torch
+
+    try:
+        p = torch.cuda.get_device_properties(dev_index)
+        return "%08X:%02X:%02X.0" % (p.pci_domain_id, p.pci_bus_id, p.pci_device_id)
+    except Exception:
+        return str(dev_index)
+
+
+def measured_hbm_peak():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per launch of the fused kernel from the committed ncu summary, if present."""
+    path = os.path.join(REPO, "profiles", "fused_grf1024_f64_k16.md")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_launch_full:"):
+                return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------- CPU runs (reference C path)
+
+def cpu_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def reference_sample(planes: int, threads: int, seed: int):
+    """Time the reference C path on a (planes+1) x 1024 x 1024 FP64 GRF slab, all 16 thresholds
+    (one reference call per threshold, as its interface takes one). Returns (seconds, voxels)."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    from oracle import RefOracle, Oracle
+
+    nz = planes + 1
+    f = grf_numpy(nz, N_SIDE, N_SIDE, seed)
+    d = (N_SIDE, N_SIDE, nz)
+    if RefOracle.available():
+        ref = RefOracle()
+        t0 = time.perf_counter()
+        for t in THRESHOLDS:
+            ref.bpfd_mt(f, d, float(t), 4, threads)
+        dt = time.perf_counter() - t0
+        kind = "reference"
+    else:  # the project's port of the same algorithm (single thread)
+        orc = Oracle()
+        view = f[: nz * N_SIDE * N_SIDE].reshape(nz, N_SIDE, N_SIDE)
+        t0 = time.perf_counter()
+        orc.bpfd_field(view, d, THRESHOLDS, [4] * K_THRESH)
+        dt = time.perf_counter() - t0
+        kind, threads = "port", 1
+    return dt, planes * N_SIDE * N_SIDE, kind, threads
+
+
+def cpu_baseline(target_s: float = 10.0):
+    threads = cpu_threads()
+    dt, vox, kind, thr = reference_sample(4, threads, SEED + 7)
+    planes = int(max(4, min(1023, 4 * target_s / max(dt, 1e-3))))
+    dt, vox, kind, thr = reference_sample(planes, threads, SEED + 7)
+    return {"value": vox / dt * 1e-9, "unit": "Gvoxel/s", "cores": thr, "kind": kind,
+            "sample": f"{planes} planes x 1024 x 1024 FP64 GRF slab, 16 thresholds (16 reference calls), "
+                      f"{dt:.2f} s"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    threads = cpu_threads()
+    # size one step to about 1 s of reference work
+    dt, vox, kind, thr = reference_sample(4, threads, SEED + 11)
+    planes = int(max(4, min(1023, 4 * 1.0 / max(dt, 1e-3))))
+    for i in range(args.warmup):
+        reference_sample(planes, threads, SEED + 100 + i)
+    times = []
+    for i in range(args.steps):
+        dt, vox, kind, thr = reference_sample(planes, threads, SEED + 200 + i)
+        times.append(dt)
+    total = sum(times)
+    value = args.steps * vox / total * 1e-9
+    line = {
+        "impl": "reference", "metric": "Gvoxel/s per field (16 thresholds)", "value": value, "unit": "Gvoxel/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "field": [N_SIDE, N_SIDE, N_SIDE], "thresholds": K_THRESH, "relation": ">",
+                   "step": f"bounded sample: {planes} planes x 1024 x 1024 per step"},
+        "cpu_baseline": {"value": value, "unit": "Gvoxel/s", "cores": thr, "kind": kind,
+                         "sample": f"{planes} planes x 1024 x 1024 FP64 GRF slab per step, 16 thresholds"},
+        "e2e": {"value": value, "unit": "Gvoxel/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- GPU run
+
+def run_mkf(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    import mkf_b200
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    mkf_b200.lib()
+    nz = N_SIDE if world == 1 else N_SIDE + 1  # with sharding, one halo plane per rank
+    f = grf_torch(nz, N_SIDE, N_SIDE, SEED + rank, dev)
+    vox = N_SIDE ** 3  # voxels of the field (or of this rank's slab) per step
+    stream = torch.cuda.current_stream(dev)
+    out = torch.zeros((K_THRESH, 256), dtype=torch.int64, device=dev)
+    meas = torch.empty((K_THRESH, 4), dtype=torch.float64, device=dev)
+    ev_k = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+
+    def step(i=None):
+        out.zero_()
+        if i is not None:
+            ev_k[i][0].record(stream)
+        mkf_b200.field_bpfd(f, THRESHOLDS, mkf_b200.BMC_GT, out=out, accumulate=True, stream=stream)
+        if i is not None:
+            ev_k[i][1].record(stream)
+        if world > 1:
+            dist.all_reduce(out)
+        mkf_b200._lib.check(mkf_b200.lib().mkfMeasuresF64Dev(meas.data_ptr(), out.data_ptr(), K_THRESH,
+                                                             stream.cuda_stream), "mkfMeasuresF64Dev")
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    sampler = ClockSampler(gpu_id_of(local_rank))
+    sampler.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    w0 = time.time()
+    e0.record(stream)
+    for i in range(args.steps):
+        step(i)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    w1 = time.time()
+    if world > 1:
+        dist.barrier()
+    time.sleep(0.1)
+    sampler.stop()
+    ms = e0.elapsed_time(e1)
+    kern_ms = float(np.mean([a.elapsed_time(b) for a, b in ev_k]))
+    t = torch.tensor([ms, kern_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms, kern_ms = float(t[0]), float(t[1])
+    value = world * vox * args.steps / (ms * 1e-3) * 1e-9
+    clocks = sampler.summary(w0, w1)
+
+    # end to end through the host-buffer entry point
+    fh = torch.empty(f.shape, dtype=f.dtype, pin_memory=True)
+    fh.copy_(f)
+    fh_np = fh.numpy()
+    del f
+    torch.cuda.empty_cache()
+    mkf_b200.field_bpfd_host(fh_np, THRESHOLDS, mkf_b200.BMC_GT)  # warm-up (staging buffers)
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        h = mkf_b200.field_bpfd_host(fh_np, THRESHOLDS, mkf_b200.BMC_GT)
+        if world > 1:
+            ht = torch.from_numpy(h.view(np.int64)).to(dev)
+            dist.all_reduce(ht)
+            h = ht.cpu().numpy()
+        mkf_b200.measures(h)
+    e2e_s = (time.perf_counter() - t0) / args.e2e_steps
+    tt = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    e2e_s = float(tt[0])
+    e2e = {"value": world * vox / e2e_s * 1e-9, "unit": "Gvoxel/s", "h2d_bytes_per_step": int(fh.numel() * 8),
+           "d2h_bytes_per_step": K_THRESH * 256 * 8}
+
+    if rank != 0:
+        return
+    peak, peak_src = measured_hbm_peak()
+    alg_bytes = vox * 8 + K_THRESH * 256 * 8
+    achieved = alg_bytes / (kern_ms * 1e-3) * 1e-9
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_source": peak_src, "traffic": profiled_traffic(), "kernel_ms": kern_ms,
+            "algorithmic_bytes": alg_bytes}
+    line = {
+        "metric": "Gvoxel/s per field (16 thresholds)", "value": value, "unit": "Gvoxel/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Gaussian random field, sigma 4, generated on the GPU)",
+        "config": {"workload": WORKLOAD, "field": [N_SIDE, N_SIDE, N_SIDE], "thresholds": K_THRESH,
+                   "threshold_range": [-2.0, 2.0], "relation": ">",
+                   "parallelism": "replicas" if world == 1 else f"z-slab shards x{world} + NCCL all-reduce of counts",
+                   "l2": "inputs 8.6 GB per step > 126 MB L2 (no flush)"},
+        "roofline": roof,
+        "e2e": e2e,
+        "gpu_launches": 2 * args.steps,
+        "clocks": clocks,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline()
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_mkf(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,97 @@
+/* mkf_b200.h - entry points that libMKF.so adds beside the original MKF interface.
+ *
+ * The original library handles one threshold per call and goes through a packed binary map in
+ * device memory. These calls fuse threshold -> pattern code -> histogram into one read of the
+ * field, take up to MKF_MAX_THRESH thresholds at once, run many fields in one launch, and
+ * return status codes instead of NULL. None of them has a counterpart in the original: the
+ * closest original calls are named beside each one.
+ *
+ * Conventions
+ *   - Pointers marked "device" must be CUDA device (or managed) memory of the current device.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream). Calls are
+ *     asynchronous with respect to the host unless stated otherwise.
+ *   - Returns MKF_OK (0) or a negative MKF_ERR_* code; mkfLastError() gives a message.
+ *   - Pattern counts are uint64_t[256] per threshold, laid out [threshold][pattern]. The pattern
+ *     code of the cell at (x,y,z) has bit i set when corner (x + (i&1), y + ((i>>1)&1),
+ *     z + ((i>>2)&1)) maps to 1, as in the original (bpfdCUDA.cuh:45-61).
+ *   - Every row of X elements contributes X-1 cells (the original double-counts rows with
+ *     X < 32; see the design notes).
+ */
+#ifndef MKF_B200_H
+#define MKF_B200_H
+#include "mkf_types.h"
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MKF_OK               0
+#define MKF_ERR_ARG         -1   /* invalid argument */
+#define MKF_ERR_CUDA        -2   /* a CUDA call failed */
+#define MKF_ERR_NOMEM       -3   /* allocation failed or over budget */
+#define MKF_ERR_TIMEOUT     -4   /* a bounded wait ran out */
+#define MKF_ERR_UNSUPPORTED -5   /* encoding / size not supported */
+#define MKF_ERR_BUSY        -6   /* queue full, try again */
+#define MKF_ERR_NOTFOUND    -7   /* unknown request tag */
+
+#define MKF_MAX_THRESH 32
+
+/* flags */
+#define MKF_F_ACCUMULATE 0x1 /* add to the output counts instead of overwriting them */
+
+/* One scalar field. stride[] holds element strides for x, y, z; all zero means planar
+ * (x fastest, no padding). enc is ENC_F32 or ENC_F64. */
+typedef struct
+{
+   const void *p;
+   NumEnc enc;
+   uint8_t pad_[3];
+   int32_t def[3];
+   int64_t stride[3];
+} MKFFieldDesc;
+
+/* A set of thresholds. Threshold k maps f to ((m_k >> (1 - (f < t_k) + (f > t_k))) & 1), with the
+ * comparison done exactly (a FP32 field is compared as if promoted to double, so thresholds are
+ * never rounded). m may be NULL, then every threshold uses mAll. */
+typedef struct
+{
+   int32_t nT;          /* 1 .. MKF_MAX_THRESH */
+   uint32_t mAll;
+   const double *t;     /* host array, nT values, any order */
+   const uint32_t *m;   /* host array or NULL */
+} MKFThreshSet;
+
+/* Last error message of the calling thread. */
+const char *mkfLastError(void);
+
+/* ---- fused single field (closest original: binMapCUDA + mkfCUDAGetBPFD, binMapCUDA.cu:144,
+ *      mkfCUDA.cu:12) ---- */
+/* One read of the field pF->p (device) gives nT pattern distributions in pBPFD (device,
+ * uint64_t[nT][256]). */
+int mkfFieldBPFD(uint64_t *pBPFD, const MKFFieldDesc *pF, const MKFThreshSet *pT, int flags, void *stream);
+
+/* The same from a HOST field: the field is copied in slabs through device staging buffers on a
+ * copy stream overlapped with the counting kernel, and the counts are copied back to pBPFDH
+ * (host, uint64_t[nT][256]). Synchronous. pF->p may be pageable or pinned host memory. */
+int mkfFieldBPFDHost(uint64_t *pBPFDH, const MKFFieldDesc *pF, const MKFThreshSet *pT);
+
+/* ---- many fields, one launch (no original counterpart; the original runs one field per call) ---- */
+/* Fields i = 0..nF-1 (device pointers) with threshold sets pT[i]; the counts of field i start at
+ * pBPFD + 256 * (nT_0 + ... + nT_{i-1}). */
+int mkfBatchBPFD(uint64_t *pBPFD, const MKFFieldDesc *pF, const MKFThreshSet *pT, int nF, int flags, void *stream);
+
+/* ---- measures (closest original: mkfSelectMeasuresBPFD, mkfUtil.c:94) ---- */
+/* For each of nSets distributions (host uint64_t[nSets][256]) write, in double:
+ *   r[4*i+0] V   = number of cells whose corner 0 is set (volume in cell units)
+ *   r[4*i+1] S   = sum over the 22 symmetry groups of gWS[g] * N_g   (surface estimate)
+ *   r[4*i+2] M   = sum of gWM[g] * N_g                                (integral mean curvature)
+ *   r[4*i+3] chi = sum of gWK[g] * N_g / 24                           (Euler characteristic)
+ * N_g = cells whose pattern is in group g; group map and weights are those of mkfUtil.c:33-58 and
+ * mkfHacks.c:9-20. */
+int mkfMeasuresF64(double *r, const uint64_t *pBPFD, int nSets);
+/* The same on the device: pBPFD and r are device pointers. */
+int mkfMeasuresF64Dev(double *r, const uint64_t *pBPFD, int nSets, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MKF_B200_H */

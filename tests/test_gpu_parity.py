@@ -1,0 +1,309 @@
+"""Parity of the CUDA library (through its C ABI) with the oracle and the reference's golden
+vectors. Integer outputs must be bit-exact; the double measures must equal the host's exactly.
+Needs a B200 (`-m gpu`)."""
+import numpy as np
+import pytest
+
+from oracle import bpfd_numpy, layout
+
+pytestmark = pytest.mark.gpu
+
+
+def to_dev(a, cuda):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(a)).to(cuda)
+
+
+def u64(t):
+    return t.cpu().numpy().view(np.uint64)
+
+
+def valid_bits_mask(X, Y, Z):
+    row, _ = layout((X, Y, Z))
+    m = np.zeros(row, np.uint32)
+    for w in range(row):
+        nb = min(32, X - 32 * w)
+        m[w] = np.uint32((1 << nb) - 1) if nb < 32 else np.uint32(0xFFFFFFFF)
+    return np.tile(m, Y * Z)
+
+
+# ---------------------------------------------------------------- fused (K thresholds, one read)
+
+def test_fused_golden_cases(mkf, golden, oracle, cuda):
+    for key in [str(n) for n in golden["names"] if not str(n).startswith("short_")]:
+        f = golden[key + "/field"]
+        t, m = golden[key + "/t"], golden[key + "/m"]
+        got = u64(mkf.field_bpfd(to_dev(f, cuda), t, m))
+        assert (got == golden[key + "/bpfd"]).all(), key
+
+
+def test_fused_short_rows(mkf, golden, oracle, cuda):
+    for key in [str(n) for n in golden["names"] if str(n).startswith("short_")]:
+        f = golden[key + "/field"]
+        Z, Y, X = f.shape
+        got = u64(mkf.field_bpfd(to_dev(f, cuda), [0.0], 4))[0]
+        assert (got == oracle.bpfd_field(f, (X, Y, Z), 0.0, 4)[0]).all(), key
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("seed", range(5))
+def test_fused_random_shapes(mkf, oracle, cuda, dtype, seed):
+    rng = np.random.default_rng(1000 + seed)
+    for _ in range(5):
+        X = int(rng.choice([1, 2, 3, 17, 31, 32, 33, 63, 64, 65, 100, 129]))
+        Y = int(rng.integers(1, 40))
+        Z = int(rng.integers(1, 80))
+        f = (rng.standard_normal((Z, Y, X)) * 1.5).astype(dtype)
+        K = int(rng.integers(1, 33))
+        t = np.sort(rng.standard_normal(K)) if seed % 2 else rng.standard_normal(K)
+        mask = int(rng.choice([4, 6, 1, 3]))
+        got = u64(mkf.field_bpfd(to_dev(f, cuda), t, mask))
+        want = oracle.bpfd_field(f, (X, Y, Z), t, mask)
+        assert (got == want).all(), (X, Y, Z, K, mask)
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_fused_mixed_relations_and_ties(mkf, oracle, cuda, seed):
+    rng = np.random.default_rng(2000 + seed)
+    X, Y, Z = 45, 23, 19
+    f = rng.integers(-3, 4, size=(Z, Y, X)).astype(np.float64) * 0.5
+    K = 12
+    t = rng.integers(-3, 4, size=K).astype(np.float64) * 0.5
+    m = rng.integers(0, 8, size=K).astype(np.uint32)
+    got = u64(mkf.field_bpfd(to_dev(f, cuda), t, m))
+    assert (got == oracle.bpfd_field(f, (X, Y, Z), t, m)).all()
+    f32 = f.astype(np.float32)
+    got = u64(mkf.field_bpfd(to_dev(f32, cuda), t, m))
+    assert (got == oracle.bpfd_field(f32, (X, Y, Z), t, m)).all()
+
+
+def test_fused_special_values(mkf, oracle, cuda):
+    rng = np.random.default_rng(7)
+    f = rng.standard_normal((9, 13, 70))
+    flat = f.ravel()
+    idx = rng.choice(flat.size, 400, replace=False)
+    flat[idx[:80]] = np.nan
+    flat[idx[80:160]] = np.inf
+    flat[idx[160:240]] = -np.inf
+    flat[idx[240:320]] = 0.0
+    flat[idx[320:]] = -0.0
+    Z, Y, X = f.shape
+    ts = [0.0, -0.0, np.inf, -np.inf, np.nan, 0.5, 1e300, -1e-300]
+    for mask in range(8):
+        got = u64(mkf.field_bpfd(to_dev(f, cuda), ts, mask))
+        assert (got == oracle.bpfd_field(f, (X, Y, Z), ts, [mask] * len(ts))).all(), mask
+        f32 = f.astype(np.float32)
+        got = u64(mkf.field_bpfd(to_dev(f32, cuda), ts, mask))
+        assert (got == oracle.bpfd_field(f32, (X, Y, Z), ts, [mask] * len(ts))).all(), mask
+
+
+def test_fused_fp32_thresholds_not_rounded(mkf, oracle, cuda):
+    """A FP32 field compared with a double threshold that no float represents: the result is
+    that of the exact comparison (as if the element were promoted to double)."""
+    f = np.full((4, 4, 40), np.float32(0.1), np.float32)
+    f[:, :, ::3] = np.nextafter(np.float32(0.1), np.float32(1))
+    t = [0.1, float(np.float32(0.1)), 0.1 + 1e-12]
+    for mask in (1, 2, 3, 4, 5, 6):
+        got = u64(mkf.field_bpfd(to_dev(f, cuda), t, mask))
+        assert (got == oracle.bpfd_field(f, (40, 4, 4), t, [mask] * 3)).all(), mask
+
+
+def test_fused_strided_view(mkf, oracle, cuda):
+    import torch
+
+    rng = np.random.default_rng(11)
+    big = rng.standard_normal((30, 40, 50))
+    v = to_dev(big, cuda)[2:27:2, 5:35, 3:47]  # non-contiguous view (Z step 2)
+    sub = np.ascontiguousarray(big[2:27:2, 5:35, 3:47])
+    Z, Y, X = sub.shape
+    got = u64(mkf.field_bpfd(v, [-0.3, 0.2, 0.9], 4))
+    assert (got == oracle.bpfd_field(sub, (X, Y, Z), [-0.3, 0.2, 0.9], 4)).all()
+    vt = to_dev(big, cuda).permute(0, 2, 1)  # x and y swapped: x stride is not 1
+    subt = np.ascontiguousarray(big.transpose(0, 2, 1))
+    Z, Y, X = subt.shape
+    got = u64(mkf.field_bpfd(vt, [0.1], 6))
+    assert (got == oracle.bpfd_field(subt, (X, Y, Z), [0.1], 6)).all()
+
+
+def test_fused_accumulate(mkf, cuda):
+    rng = np.random.default_rng(3)
+    f = to_dev(rng.standard_normal((20, 30, 40)), cuda)
+    a = mkf.field_bpfd(f, [0.0, 0.5], 4)
+    b = mkf.field_bpfd(f, [0.0, 0.5], 4, out=a.clone(), accumulate=True)
+    assert (u64(b) == 2 * u64(a)).all()
+
+
+# ---------------------------------------------------------------- size-independent properties at full size
+
+def test_full_size_multi_threshold_properties(mkf, oracle, cuda):
+    """1024^3 FP64, 16 thresholds in [-2, 2]: every distribution sums to the cell count; '>' and
+    '<=' are complements; counting two z-slabs sharing a plane gives the full counts; a 64^3
+    block matches the oracle exactly."""
+    import torch
+
+    n = 1024
+    g = torch.Generator(device=cuda).manual_seed(5)
+    f = torch.randn((n, n, n), dtype=torch.float64, device=cuda, generator=g)
+    f = (f + f.roll(1, 0) + f.roll(1, 1) + f.roll(1, 2)) * 0.5  # some spatial correlation
+    t = np.linspace(-2, 2, 16)
+    h_gt = u64(mkf.field_bpfd(f, t, 4))
+    cells = (n - 1) ** 3
+    assert (h_gt.sum(axis=1) == cells).all()
+    h_le = u64(mkf.field_bpfd(f, t, 3))
+    assert (h_le == h_gt[:, ::-1]).all()
+    h_a = u64(mkf.field_bpfd(f[:600], t, 4))
+    h_b = u64(mkf.field_bpfd(f[599:], t, 4))
+    assert (h_a + h_b == h_gt).all()
+    # all-ones counts fall and all-zero counts rise with the threshold
+    assert (np.diff(h_gt[:, 255].astype(np.int64)) <= 0).all()
+    assert (np.diff(h_gt[:, 0].astype(np.int64)) >= 0).all()
+    blk = f[100:164, 300:364, 700:764].contiguous()
+    hb = u64(mkf.field_bpfd(blk, t, 4))
+    assert (hb == oracle.bpfd_field(blk.cpu().numpy(), (64, 64, 64), t, 4)).all()
+    del f
+
+
+# ---------------------------------------------------------------- drop-in: binMapCUDA + mkfCUDAGetBPFD
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_dropin_golden(mkf, golden, cuda, dtype):
+    for key in [str(n) for n in golden["names"] if not str(n).startswith("short_")]:
+        f = golden[key + "/field"].astype(dtype)
+        Z, Y, X = f.shape
+        vm = valid_bits_mask(X, Y, Z)
+        for k, (t, m) in enumerate(zip(golden[key + "/t"], golden[key + "/m"])):
+            if np.isinf(t):
+                continue
+            rel = {1: "<", 2: "=", 3: "<=", 4: ">", 5: "!=", 6: ">=", 7: "<=>", 0: ""}[int(m)]
+            pbm, org, ki = mkf.bin_map_cuda(to_dev(f, cuda), rel, float(t))
+            words = pbm.cpu().numpy().view(np.uint32)[: vm.size]
+            if dtype == np.float64 or key.startswith("int_"):
+                assert ((words & vm) == (golden[key + "/pbm"][k] & vm)).all(), (key, k)
+                assert (mkf.get_bpfd_host(pbm, org) == golden[key + "/bpfd"][k]).all(), (key, k)
+            pad = words & ~vm
+            assert (pad == 0).all()
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_dropin_random_vs_oracle(mkf, oracle, cuda, seed):
+    rng = np.random.default_rng(3000 + seed)
+    for _ in range(6):
+        X = int(rng.choice([5, 31, 32, 33, 64, 70, 200]))
+        Y, Z = int(rng.integers(2, 30)), int(rng.integers(2, 30))
+        dtype = [np.float32, np.float64][seed % 2]
+        f = rng.standard_normal((Z, Y, X)).astype(dtype)
+        t = float(np.float32(rng.standard_normal()))
+        pbm, org, _ = mkf.bin_map_cuda(to_dev(f, cuda), ">", t)
+        assert (org.rowElem, org.rowPairs, org.planePairs) == (X, Y - 1, Z - 1)
+        want_map = oracle.pack(f, (X, Y, Z), t, 4)
+        assert (pbm.cpu().numpy().view(np.uint32)[: want_map.size] == want_map).all()
+        want = oracle.bpfd_field(f, (X, Y, Z), t, 4)[0]
+        assert (mkf.get_bpfd_host(pbm, org) == want).all()
+        # mkfCUDAGetBPFD accumulates into the caller's device array
+        acc = mkf.get_bpfd(pbm, org)
+        acc = mkf.get_bpfd(pbm, org, out=acc)
+        assert (u64(acc) == 2 * want).all()
+
+
+def test_dropin_multi_field_sum_and_strides(mkf, oracle, cuda):
+    import torch
+
+    rng = np.random.default_rng(17)
+    for dtype in (np.float32, np.float64):
+        fs = [rng.standard_normal((11, 13, 45)).astype(dtype) for _ in range(3)]
+        pbm, org, _ = mkf.bin_map_cuda([to_dev(a, cuda) for a in fs], ">=", 0.25)
+        want = oracle.pack(fs, (45, 13, 11), 0.25, 6)
+        assert (pbm.cpu().numpy().view(np.uint32)[: want.size] == want).all()
+    # element strides given explicitly: a (Z, Y, X) view inside a larger array
+    big = rng.standard_normal((12, 20, 70)).astype(np.float64)
+    d = to_dev(big, cuda)
+    view = d[1:11, 2:18, 5:60]
+    sub = np.ascontiguousarray(big[1:11, 2:18, 5:60])
+    pbm, org, _ = mkf.bin_map_cuda(view, ">", 0.1, strides_zyx=view.stride())
+    want = oracle.pack(sub, (55, 16, 10), 0.1, 4)
+    assert (pbm.cpu().numpy().view(np.uint32)[: want.size] == want).all()
+
+
+def test_dropin_unit_dimensions_collapse(mkf, oracle, cuda):
+    rng = np.random.default_rng(19)
+    f = rng.standard_normal((40, 33, 1))  # X = 1: the map is laid out as 33 x 40 x 1
+    pbm, org, _ = mkf.bin_map_cuda(to_dev(f, cuda), ">", 0.0)
+    assert (org.rowElem, org.rowPairs, org.planePairs) == (33, 39, 0)
+    want = oracle.pack(f.reshape(1, 40, 33), (33, 40, 1), 0.0, 4)
+    assert (pbm.cpu().numpy().view(np.uint32)[: want.size] == want).all()
+    assert (mkf.get_bpfd_host(pbm, org) == 0).all()
+
+
+def test_dropin_auto_context(mkf, oracle, cuda):
+    import ctypes as C
+
+    rng = np.random.default_rng(23)
+    X, Y, Z = 64, 20, 12
+    f = rng.standard_normal((Z, Y, X)).astype(np.float32)
+    L = mkf.lib()
+    ctx = mkf._lib.Context()
+    ctx.nField, ctx.nElem, ctx.enc, ctx.bytesElem = 1, X * Y * Z, mkf.ENC_F32, 4
+    ctx.bytesF = f.nbytes
+    words = L.setBMO(C.byref(ctx.bmo), (C.c_int * 3)(X, Y, Z), b"\x00")
+    ctx.nU, ctx.bytesU = words, words * 4
+    ctx.nZ, ctx.bytesZ = 256, 2048
+    assert L.cuBuffAlloc(C.byref(ctx), 0) == 1
+    C.memmove(ctx.pHF, f.ctypes.data, f.nbytes)
+    bm = mkf.BinMapF64()
+    L.setBinMapF64(C.byref(bm), b">", 0.0)
+    assert L.mkfCUDAGetBPFDautoCtx(C.byref(ctx), (C.c_int * 3)(X, Y, Z), C.byref(bm), 0) == 1
+    got_map = np.ctypeslib.as_array(C.cast(ctx.pHU, C.POINTER(C.c_uint32)), shape=(words,)).copy()
+    assert (got_map == oracle.pack(f, (X, Y, Z), 0.0, 4)).all()
+    # second stage: counts from the packed map already in the context
+    pHF = ctx.pHF
+    ctx.pHF = None
+    assert L.mkfCUDAGetBPFDautoCtx(C.byref(ctx), (C.c_int * 3)(X, Y, Z), C.byref(bm), 0) == 1
+    got = np.ctypeslib.as_array(C.cast(ctx.pHZ, C.POINTER(C.c_uint64)), shape=(256,)).copy()
+    assert (got == oracle.bpfd_field(f, (X, Y, Z), 0.0, 4)[0]).all()
+    ctx.pHF = pHF
+    assert L.cuBuffRelease(C.byref(ctx)) == 1
+    L.mkfCUDACleanup(1)
+    L.binMapCUDACleanup()
+
+
+# ---------------------------------------------------------------- host path, batch, measures
+
+def test_host_field_path(mkf, oracle, cuda):
+    rng = np.random.default_rng(29)
+    # (40, 1024, 2048) FP32 has 8 MB planes, so the field is staged in two slabs
+    for dtype, shape in [(np.float32, (300, 90, 101)), (np.float64, (5, 7, 33)), (np.float64, (1, 7, 33)),
+                         (np.float32, (40, 1024, 2048))]:
+        f = rng.standard_normal(shape).astype(dtype)
+        Z, Y, X = shape
+        t = [-1.0, 0.0, 0.7]
+        got = mkf.field_bpfd_host(f, t, 4)
+        dev = u64(mkf.field_bpfd(to_dev(f, cuda), t, 4))
+        assert (got == dev).all()
+        if f.size < 100000:
+            assert (got == oracle.bpfd_field(f, (X, Y, Z), t, 4)).all()
+
+
+def test_batch_equals_per_field(mkf, cuda):
+    rng = np.random.default_rng(31)
+    fields, ts = [], []
+    for _ in range(9):
+        shape = tuple(int(v) for v in rng.integers(17, 60, size=3))
+        dtype = (np.float32, np.float64)[int(rng.integers(0, 2))]
+        fields.append(to_dev(rng.standard_normal(shape).astype(dtype), cuda))
+        ts.append(np.sort(rng.standard_normal(int(rng.integers(1, 9)))))
+    got = u64(mkf.batch_bpfd(fields, ts))
+    row = 0
+    for f, t in zip(fields, ts):
+        want = u64(mkf.field_bpfd(f, t, 4))
+        assert (got[row:row + len(t)] == want).all()
+        row += len(t)
+
+
+def test_device_measures_equal_host(mkf, golden, cuda):
+    import torch
+
+    hs = np.concatenate([golden[str(k) + "/bpfd"] for k in golden["names"] if not str(k).startswith("short_")])
+    dev = mkf.measures_dev(torch.from_numpy(hs.view(np.int64)).to(cuda)).cpu().numpy()
+    host = mkf.measures(hs)
+    assert (dev == host).all()
