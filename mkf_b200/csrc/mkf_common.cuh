@@ -25,8 +25,8 @@ static constexpr unsigned FULL = 0xFFFFFFFFu;
 template <typename T>
 __device__ __forceinline__ unsigned relIdx(T f, T t) { return 1u - (f < t) + (f > t); }
 
-// Bits [0, r) set, r in [0, 32].
-__device__ __forceinline__ uint32_t thermo(uint32_t r) { return __funnelshift_lc(0u, 0xFFFFFFFFu, r) ; }
+// Bits [0, r) set, r in [0, 32]: the upper word of (0 : 0xFFFFFFFF) << min(r, 32).
+__device__ __forceinline__ uint32_t thermo(uint32_t r) { return __funnelshift_lc(0xFFFFFFFFu, 0u, r); }
 
 // Bit-sliced counter of per-bit-position sums of 32-bit words, via a carry-save (Harley-Seal)
 // tree: add() takes words one at a time; each bit position k of the words is summed
