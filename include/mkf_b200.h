@@ -74,6 +74,25 @@ int mkfFieldBPFD(uint64_t *pBPFD, const MKFFieldDesc *pF, const MKFThreshSet *pT
  * (host, uint64_t[nT][256]). Synchronous. pF->p may be pageable or pinned host memory. */
 int mkfFieldBPFDHost(uint64_t *pBPFDH, const MKFFieldDesc *pF, const MKFThreshSet *pT);
 
+/* The same as mkfFieldBPFDHost, but the library allocates nothing: no cudaMalloc, no pinned
+ * buffers, no streams or events. It has no counterpart in the original MKF.
+ *   Who needs it: callers that must not let a library allocate device memory, such as an in-situ
+ *   analysis inside a simulation whose device memory belongs to the simulation's own pool, or a
+ *   process held to a fixed device-memory budget (cudaMalloc would also synchronise the device
+ *   in the middle of the caller's overlapped work).
+ *   Scratch: two file-scope device arrays of the library, a 32 MiB staging area for field slabs
+ *   and 32 x 256 counts; every GPU that loads the library holds them until the process exits.
+ *   Limit: the staging area must hold two planes, so a plane (X * Y elements) may be at most
+ *   16 MiB (e.g. 2048 x 1024 FP64, 2048 x 2048 FP32); larger planes return MKF_ERR_NOMEM.
+ *   The first call on each device resolves the arrays' device addresses (cudaGetSymbolAddress)
+ *   with that device current; make that first call before any stream capture.
+ *   All calls on a device share the arrays: calls whose work overlaps on the GPU (different
+ *   streams, or different host threads) race and give wrong counts. The counts are cleared at
+ *   the start of every call; the staging area keeps the last call's data.
+ *   Work runs in order on `stream` (NULL = legacy default stream); returns after the counts are
+ *   in pBPFDH (host, uint64_t[nT][256]). pF->p is a planar host field. */
+int mkfFieldBPFDHostNoAlloc(uint64_t *pBPFDH, const MKFFieldDesc *pF, const MKFThreshSet *pT, void *stream);
+
 /* ---- many fields, one launch (no original counterpart; the original runs one field per call) ---- */
 /* Fields i = 0..nF-1 (device pointers) with threshold sets pT[i]; the counts of field i start at
  * pBPFD + 256 * (nT_0 + ... + nT_{i-1}). */

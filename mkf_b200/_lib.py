@@ -103,6 +103,7 @@ _SIG = [
     ("mkfLastError", C.c_char_p, []),
     ("mkfFieldBPFD", C.c_int, [_P, C.POINTER(MKFFieldDesc), C.POINTER(MKFThreshSet), C.c_int, _P]),
     ("mkfFieldBPFDHost", C.c_int, [_P, C.POINTER(MKFFieldDesc), C.POINTER(MKFThreshSet)]),
+    ("mkfFieldBPFDHostNoAlloc", C.c_int, [_P, C.POINTER(MKFFieldDesc), C.POINTER(MKFThreshSet), _P]),
     ("mkfBatchBPFD", C.c_int, [_P, C.POINTER(MKFFieldDesc), C.POINTER(MKFThreshSet), C.c_int, C.c_int, _P]),
     ("mkfMeasuresF64", C.c_int, [_P, _P, C.c_int]),
     ("mkfMeasuresF64Dev", C.c_int, [_P, _P, C.c_int, _P]),

@@ -316,6 +316,40 @@ static void floatBounds(double t, double &tlo, double &thi)
    thi = b;
 }
 
+// Plain-argument launch of one fused pass, for callers that must not touch the heap. The
+// thresholds are already sorted and converted (tlo/thi as the kernel compares them).
+int launchFusedPlain(const FusedPlain &q, cudaStream_t s)
+{
+   FusedArgs a;
+   memset(&a, 0, sizeof(a));
+   a.f = q.f;
+   a.sx = q.sx; a.sy = q.sy; a.sz = q.sz;
+   a.X = q.X; a.Y = q.Y; a.Z = q.Z;
+   a.K = q.K;
+   for (int i = 0; i < 64; i++) { a.tlo[i] = INFINITY; a.thi[i] = INFINITY; }
+   for (int k = 0; k < q.K; k++) { a.tlo[k] = q.tlo[k]; a.thi[k] = q.thi[k]; a.outRow[k] = q.outRow[k]; }
+   a.gtm = q.gtm; a.eqm = q.eqm; a.ltm = q.ltm; a.nanP = q.eqm;
+   a.nanRank = q.nanRank; a.rankHi = q.rankHi; a.complement = q.complement;
+   a.out = q.out;
+   constexpr int TY = 16;
+   a.D = 64;
+   a.nSegX = (q.X - 1 + 30) / 31;
+   a.nTileY = (q.Y - 1 + TY - 1) / TY;
+   a.nSlabZ = (q.Z - 1 + a.D - 1) / a.D;
+   a.nItems = (long long)a.nSegX * a.nTileY * a.nSlabZ;
+   const bool f32 = q.enc == ENC_F32;
+   if (q.thermo) { return f32 ? dispatchLevels<float, TY, true>(a, s) : dispatchLevels<double, TY, true>(a, s); }
+   return f32 ? dispatchLevels<float, TY, false>(a, s) : dispatchLevels<double, TY, false>(a, s);
+}
+
+int launchConstBin(uint64_t *out, int row, int bin, unsigned long long cells, cudaStream_t s)
+{
+   addConstBin<<<1, 1, 0, s>>>(out, row, bin, cells);
+   return cudaFail(cudaGetLastError(), "addConstBin launch");
+}
+
+void floatBoundsPlain(double t, double &tlo, double &thi) { floatBounds(t, tlo, thi); }
+
 int fieldBPFD(uint64_t *out, const MKFFieldDesc *pF, const MKFThreshSet *pT, int flags, cudaStream_t s,
               const int *rowBase /* output row of threshold i, NULL = identity */)
 {

@@ -90,3 +90,23 @@ struct SliceCounter
 };
 
 }  // namespace mkf
+
+namespace mkf {
+// One fused counting pass in plain arguments (see launchFusedPlain in fused.cu).
+struct FusedPlain
+{
+   const void *f;
+   int enc;
+   int64_t sx, sy, sz;
+   int X, Y, Z;
+   int K;
+   double tlo[MKF_MAX_THRESH], thi[MKF_MAX_THRESH];
+   int outRow[MKF_MAX_THRESH];
+   uint32_t gtm, eqm, ltm, nanRank;
+   int thermo, rankHi, complement;
+   uint64_t *out;
+};
+int launchFusedPlain(const FusedPlain &q, cudaStream_t s);
+int launchConstBin(uint64_t *out, int row, int bin, unsigned long long cells, cudaStream_t s);
+void floatBoundsPlain(double t, double &tlo, double &thi);
+}  // namespace mkf
