@@ -26,28 +26,9 @@
 #include <cstring>
 #include <mutex>
 #include <vector>
-#include "mkf_common.cuh"
+#include "fused.cuh"
 
 namespace mkf {
-
-struct FusedArgs
-{
-   const void *f;
-   int64_t sx, sy, sz;   // element strides
-   int X, Y, Z;
-   int K;                // thresholds in this pass (sorted ascending)
-   int D;                // planes of cells per slab
-   int nSegX, nTileY, nSlabZ;
-   long long nItems;     // nSegX * nTileY * nSlabZ warp work items
-   uint32_t gtm, eqm, ltm, nanP;  // GEN: per-threshold relation bits, map word of a NaN element
-   uint32_t nanRank;     // THERMO: rank of a NaN element
-   int rankHi;           // THERMO: rank counts thresholds <= f (else < f)
-   int complement;       // THERMO: stored codes are the bitwise complement of the true codes
-   uint64_t *out;        // [.][256] distributions
-   int outRow[MKF_MAX_THRESH];  // output row of sorted threshold k
-   double tlo[64];       // sorted thresholds for the "f > t" test, +inf padded
-   double thi[64];       // sorted thresholds for the "f >= t" test, +inf padded
-};
 
 static constexpr int kWarps = 8;
 
@@ -338,7 +319,12 @@ int launchFusedPlain(const FusedPlain &q, cudaStream_t s)
    a.nSlabZ = (q.Z - 1 + a.D - 1) / a.D;
    a.nItems = (long long)a.nSegX * a.nTileY * a.nSlabZ;
    const bool f32 = q.enc == ENC_F32;
-   if (q.thermo) { return f32 ? dispatchLevels<float, TY, true>(a, s) : dispatchLevels<double, TY, true>(a, s); }
+   if (q.thermo) {
+      FusedArgs b = a;
+      const int rc = launchThermo(b, q.enc, s);
+      if (rc != MKF_ERR_UNSUPPORTED) { return rc; }
+      return f32 ? dispatchLevels<float, TY, true>(a, s) : dispatchLevels<double, TY, true>(a, s);
+   }
    return f32 ? dispatchLevels<float, TY, false>(a, s) : dispatchLevels<double, TY, false>(a, s);
 }
 
@@ -449,7 +435,13 @@ int fieldBPFD(uint64_t *out, const MKFFieldDesc *pF, const MKFThreshSet *pT, int
       a.nSlabZ = (Z - 1 + a.D - 1) / a.D;
       a.nItems = (long long)a.nSegX * a.nTileY * a.nSlabZ;
       const bool f32 = pF->enc == ENC_F32;
-      if (ps.thermo) { rc = f32 ? dispatchLevels<float, TY, true>(a, s) : dispatchLevels<double, TY, true>(a, s); }
+      if (ps.thermo) {
+         FusedArgs b = a;
+         rc = launchThermo(b, pF->enc, s);
+         if (rc == MKF_ERR_UNSUPPORTED) {
+            rc = f32 ? dispatchLevels<float, TY, true>(a, s) : dispatchLevels<double, TY, true>(a, s);
+         }
+      }
       else { rc = f32 ? dispatchLevels<float, TY, false>(a, s) : dispatchLevels<double, TY, false>(a, s); }
       if (rc != MKF_OK) { return rc; }
    }

@@ -30,7 +30,7 @@ __device__ __forceinline__ uint32_t thermo(uint32_t r) { return __funnelshift_lc
 
 // Bit-sliced counter of per-bit-position sums of 32-bit words, via a carry-save (Harley-Seal)
 // tree: add() takes words one at a time; each bit position k of the words is summed
-// independently. Exact up to 2^(4+HI) - 1 words between flushes.
+// independently. Exact up to 16 * (2^HI - 1) + 15 words between flushes.
 template <int HI>
 struct SliceCounter
 {

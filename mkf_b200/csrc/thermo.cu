@@ -1,0 +1,369 @@
+// thermo.cu - fused counting kernel for threshold sets that share one relation (< <= > >=).
+//
+// Sorted thresholds make an element's K map bits a thermometer, bits[k] = (k < rank), so an
+// element reduces to one rank 0..K. The rank is found with a table over order-preserving 32-bit
+// keys: key(f) orders like f, the table maps key >> 18 (16384 buckets) to the number of
+// threshold keys below the bucket, and one compare with the bucket's only candidate threshold
+// finishes the count. FP32 keys are exact. A FP64 element is read as its high word only (same
+// DRAM sectors, half the load bandwidth into the SM); when that word ties with the candidate's or
+// the element is inf/NaN, the element is re-read whole and ranked exactly by binary search.
+//
+// A warp owns 32 x positions (31 cells, neighbouring columns overlap by one element), TY rows and
+// D planes; it walks the planes, keeping per row pair of the previous plane the four corner ranks
+// (one byte each) and their min | max << 8. A cell's pattern for threshold k is all-ones for
+// k < min rank, all-zeros for k >= max rank, and is formed with byte arithmetic on the two faces'
+// packed ranks only for k in between; those codes go to the per-CTA [K][256] shared histogram.
+// All-ones counts are summed per threshold with bit-sliced carry-save adders and all-zeros counts
+// follow from the number of cells, as in fused.cu.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include "fused.cuh"
+
+namespace mkf {
+
+static constexpr int kThWarps = 8;
+static constexpr int kLutShift = 18;
+static constexpr int kLutSize = 1 << (32 - kLutShift);
+
+// Order-preserving map of IEEE bits to unsigned: negative values reversed below positive ones.
+__host__ __device__ __forceinline__ uint32_t sortKey(uint32_t u)
+{
+   return u ^ ((uint32_t)((int32_t)u >> 31) | 0x80000000u);
+}
+
+// The 32-bit word ranked on the fast path: the whole float, or the high word of a double.
+template <typename T>
+__device__ __forceinline__ uint32_t loadWord(const T *__restrict__ F, long long i);
+template <>
+__device__ __forceinline__ uint32_t loadWord<float>(const float *__restrict__ F, long long i)
+{
+   return __ldg(reinterpret_cast<const unsigned *>(F) + i);
+}
+template <>
+__device__ __forceinline__ uint32_t loadWord<double>(const double *__restrict__ F, long long i)
+{
+   return __ldg(reinterpret_cast<const unsigned *>(F) + 2 * i + 1);
+}
+
+// Asynchronous 4-byte global -> shared copy (completes at cp.async.wait_group).
+__device__ __forceinline__ void cpAsync4(uint32_t *dst, const unsigned *src)
+{
+   const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cpAsyncWait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Exact rank of the element F[i] by binary search over the sorted thresholds in the field's
+// precision. Kept out of line: it runs only for the rare elements the fast path cannot decide.
+template <typename T, bool GE>
+__device__ __noinline__ uint32_t exactRank(const T *__restrict__ F, long long i, const T *sTlo, const T *sThi, int K,
+                                           uint32_t nanRank)
+{
+   const T v = __ldg(F + i);
+   uint32_t r = 0;
+#pragma unroll
+   for (int s = 32; s >= 1; s >>= 1) {
+      if (v > sTlo[r + s - 1]) { r += s; }
+   }
+   if (r > (uint32_t)K) { r = K; }
+   if (GE) {
+      while (r < (uint32_t)K && v >= sThi[r]) { ++r; }
+   }
+   return (v != v) ? nanRank : r;
+}
+
+// Carry-save accumulation of the 16 all-ones words of one plane (one per row pair), as a fixed
+// tree: every word enters at its row index, so no branch depends on a run-time count.
+struct PlaneOnes
+{
+   uint32_t ones = 0, twos = 0, fours = 0, eights = 0;
+   uint32_t hi[6] = {0, 0, 0, 0, 0, 0};  // sixteens, bit-sliced (up to 63 planes' worth)
+   uint32_t p1 = 0, p2 = 0, p4 = 0, p8 = 0;
+   __device__ __forceinline__ static void fa(uint32_t &s, uint32_t &c, uint32_t a, uint32_t b, uint32_t d)
+   {
+      s = a ^ b ^ d;
+      c = (a & b) | (d & (a ^ b));
+   }
+   // j is the row index 0..15; called from a fully unrolled loop, so every test on j folds away
+   __device__ __forceinline__ void add(const int J, uint32_t w)
+   {
+      if ((J & 1) == 0) { p1 = w; return; }
+      uint32_t c2, c4, c8, c16;
+      fa(ones, c2, ones, p1, w);
+      if ((J & 2) == 0) { p2 = c2; return; }
+      fa(twos, c4, twos, p2, c2);
+      if ((J & 4) == 0) { p4 = c4; return; }
+      fa(fours, c8, fours, p4, c4);
+      if ((J & 8) == 0) { p8 = c8; return; }
+      fa(eights, c16, eights, p8, c8);
+#pragma unroll
+      for (int i = 0; i < 6; i++) {
+         const uint32_t t = hi[i] & c16;
+         hi[i] ^= c16;
+         c16 = t;
+      }
+   }
+   __device__ __forceinline__ uint32_t total(int k) const
+   {
+      uint32_t v = ((ones >> k) & 1u) + 2u * ((twos >> k) & 1u) + 4u * ((fours >> k) & 1u) + 8u * ((eights >> k) & 1u);
+#pragma unroll
+      for (int i = 0; i < 6; i++) { v += (16u << i) * ((hi[i] >> k) & 1u); }
+      return v;
+   }
+};
+
+template <typename T, int TY, bool GE>
+__global__ void __launch_bounds__(kThWarps * 32, 2) thermoBPFD(const __grid_constant__ FusedArgs a)
+{
+   static_assert(TY == 16, "the all-ones tree takes 16 rows per plane");
+   constexpr int W = sizeof(T) / 4;  // 32-bit words per element; the ranked word is the last one
+   __shared__ uint8_t sLut[kLutSize];
+   __shared__ uint32_t sKey[MKF_MAX_THRESH + 1];
+   __shared__ T sTlo[64];
+   __shared__ T sThi[64];
+   __shared__ uint32_t sOnes[MKF_MAX_THRESH];
+   __shared__ unsigned long long sCells;
+   // dynamic shared memory: per warp, two planes of the 32-bit words each lane ranks
+   // ([warp][buffer][row][lane]), then the [K][256] histogram
+   extern __shared__ uint32_t sDyn[];
+   uint32_t *sHist = sDyn + kThWarps * 2 * (TY + 1) * 32;
+
+   const int K = a.K;
+   for (int i = threadIdx.x; i < K * 256; i += blockDim.x) { sHist[i] = 0; }
+   for (int i = threadIdx.x; i < 64; i += blockDim.x) {
+      sTlo[i] = (T)a.tlo[i];
+      sThi[i] = (T)a.thi[i];
+   }
+   for (int i = threadIdx.x; i <= MKF_MAX_THRESH; i += blockDim.x) { sKey[i] = (i < K) ? a.tkey[i] : 0xFFFFFFFFu; }
+   // bucket b -> number of threshold keys below the bucket's first key
+   for (int b = threadIdx.x; b < kLutSize; b += blockDim.x) {
+      const uint32_t start = (uint32_t)b << kLutShift;
+      uint32_t n = 0;
+      for (int k = 0; k < K; k++) { n += a.tkey[k] < start; }
+      sLut[b] = (uint8_t)n;
+   }
+   if (threadIdx.x < MKF_MAX_THRESH) { sOnes[threadIdx.x] = 0; }
+   if (threadIdx.x == 0) { sCells = 0; }
+   __syncthreads();
+
+   const int lane = threadIdx.x & 31;
+   uint32_t(*stage)[TY + 1][32] = reinterpret_cast<uint32_t(*)[TY + 1][32]>(sDyn + (threadIdx.x >> 5) * 2 * (TY + 1) * 32);
+   const long long gw = (long long)blockIdx.x * kThWarps + (threadIdx.x >> 5);
+   const long long nw = (long long)gridDim.x * kThWarps;
+   const unsigned *__restrict__ F32w = reinterpret_cast<const unsigned *>(a.f) + (W - 1);
+   const long long rowStep = (long long)W * a.sy, planeStep = (long long)W * a.sz;
+   const uint32_t nanRank = a.nanRank;
+   unsigned long long cells = 0;
+
+   for (long long it = gw; it < a.nItems; it += nw) {
+      const int ix = (int)(it % a.nSegX);
+      const long long rest = it / a.nSegX;
+      const int iy = (int)(rest % a.nTileY);
+      const int iz = (int)(rest / a.nTileY);
+      const int x0 = 31 * ix, y0 = TY * iy, z0 = a.D * iz;
+      const int xl = min(x0 + lane, a.X - 1);  // lanes past the row end re-read the last element
+      const uint32_t vx = ((lane < 31) && (x0 + lane < a.X - 1)) ? 0xFFFFFFFFu : 0u;
+      const int nRow = min(TY, a.Y - 1 - y0);
+      const int nPln = min(a.D, a.Z - 1 - z0);
+      cells += (unsigned long long)max(0, min(31, a.X - 1 - x0)) * (unsigned)nRow * (unsigned)nPln;
+      const int lastRow = a.Y - 1 - y0;  // rows j > lastRow re-read row lastRow
+      // word offsets of the TY+1 rows relative to the row y0 (clamped), kept as 32-bit steps
+      const unsigned *__restrict__ P = F32w + (long long)W * ((long long)xl * a.sx + (long long)y0 * a.sy + (long long)z0 * a.sz);
+
+      // stage plane 0; every lane later reads back only the words it copied itself
+      {
+         const unsigned *q = P;
+#pragma unroll
+         for (int j = 0; j <= TY; ++j) {
+            cpAsync4(&stage[0][j][lane], q);
+            if (j < lastRow) { q += rowStep; }
+         }
+         cpAsyncCommit();
+      }
+      uint32_t sF[TY], sM[TY];  // previous plane: face ranks, min | max << 8 per row pair
+      PlaneOnes ones;
+      for (int p = 0; p <= nPln; ++p) {
+         P += planeStep;
+         if (p < nPln) {  // stage the next plane while this one is ranked and counted
+            const unsigned *q = P;
+#pragma unroll
+            for (int j = 0; j <= TY; ++j) {
+               cpAsync4(&stage[(p + 1) & 1][j][lane], q);
+               if (j < lastRow) { q += rowStep; }
+            }
+            cpAsyncCommit();
+            cpAsyncWait<1>();
+         } else {
+            cpAsyncWait<0>();
+         }
+         const uint32_t(*w)[32] = stage[p & 1];
+         uint32_t r[TY + 1];
+         uint32_t slow = 0;  // bit j: element of row j needs the exact rank
+#pragma unroll
+         for (int j = 0; j <= TY; ++j) {
+            const uint32_t wj = w[j][lane];
+            const uint32_t key = sortKey(wj);
+            const uint32_t r0 = sLut[key >> kLutShift];
+            const uint32_t cand = sKey[r0];
+            r[j] = r0 + (GE ? (key >= cand) : (key > cand));
+            if (W == 2) {
+               slow |= (uint32_t)((key == cand) | ((key - 0x00100000u) >= 0xFFE00000u)) << j;
+            } else {
+               r[j] = ((wj & 0x7FFFFFFFu) > 0x7F800000u) ? nanRank : r[j];
+            }
+         }
+         if (W == 2 && slow) {
+            const T *Fe = reinterpret_cast<const T *>(a.f);
+            const long long e0 = (long long)xl * a.sx + (long long)y0 * a.sy + (long long)(z0 + p) * a.sz;
+#pragma unroll
+            for (int j = 0; j <= TY; ++j) {
+               if ((slow >> j) & 1u) {
+                  r[j] = exactRank<T, GE>(Fe, e0 + (long long)min(j, lastRow) * a.sy, sTlo, sThi, K, nanRank);
+               }
+            }
+         }
+         uint32_t rR = __shfl_down_sync(FULL, r[0], 1);
+         uint32_t ePrev = __byte_perm(r[0], rR, 0x0040);
+         uint32_t mnPrev = min(r[0], rR), mxPrev = max(r[0], rR);
+         if (p == 0) {
+#pragma unroll
+            for (int j = 0; j < TY; ++j) {
+               rR = __shfl_down_sync(FULL, r[j + 1], 1);
+               const uint32_t e = __byte_perm(r[j + 1], rR, 0x0040);
+               const uint32_t mn = min(r[j + 1], rR), mx = max(r[j + 1], rR);
+               sF[j] = __byte_perm(ePrev, e, 0x5410);
+               sM[j] = min(mnPrev, mn) | (max(mxPrev, mx) << 8);
+               ePrev = e;
+               mnPrev = mn;
+               mxPrev = mx;
+            }
+            continue;
+         }
+#pragma unroll
+         for (int j = 0; j < TY; ++j) {
+            rR = __shfl_down_sync(FULL, r[j + 1], 1);
+            const uint32_t e = __byte_perm(r[j + 1], rR, 0x0040);
+            const uint32_t mn = min(r[j + 1], rR), mx = max(r[j + 1], rR);
+            const uint32_t fc = __byte_perm(ePrev, e, 0x5410);
+            const uint32_t fmn = min(mnPrev, mn), fmx = max(mxPrev, mx);
+            const uint32_t rmin = min(sM[j] & 0xFFu, fmn);
+            const uint32_t vmask = (j < nRow) ? vx : 0u;
+            const uint32_t rmax = vmask ? max(sM[j] >> 8, fmx) : rmin;  // invalid cells: no mixed codes
+            ones.add(j, thermo(rmin) & vmask);
+            if (rmin < rmax) {
+               const uint32_t R0 = sF[j], R1 = fc;
+               uint32_t C = 0x7F7F7F7Fu - rmin * 0x01010101u;
+               uint32_t *h = sHist + (rmin << 8);
+               uint32_t k = rmin;
+               do {
+                  const uint32_t t0 = (R0 + C) & 0x80808080u;
+                  const uint32_t t1 = (R1 + C) & 0x80808080u;
+                  const uint32_t c = ((t0 * 0x00204081u) >> 28) | (((t1 * 0x00204081u) >> 24) & 0xF0u);
+                  atomicAdd(h + c, 1u);
+                  C -= 0x01010101u;
+                  h += 256;
+               } while (++k < rmax);
+            }
+            sF[j] = fc;
+            sM[j] = fmn | (fmx << 8);
+            ePrev = e;
+            mnPrev = mn;
+            mxPrev = mx;
+         }
+      }
+      for (int k = 0; k < K; ++k) {
+         const uint32_t s = __reduce_add_sync(FULL, ones.total(k));
+         if (lane == 0 && s) { atomicAdd(&sOnes[k], s); }
+      }
+   }
+   if (lane == 0 && cells) { atomicAdd(&sCells, cells); }
+   __syncthreads();
+
+   const int warp = threadIdx.x >> 5;
+   for (int k = warp; k < K; k += kThWarps) {
+      uint32_t s = 0;
+      for (int c = 1 + lane; c < 255; c += 32) { s += sHist[k * 256 + c]; }
+      s = __reduce_add_sync(FULL, s);
+      if (lane == 0) {
+         const unsigned long long n1 = sOnes[k];
+         const unsigned long long n0 = sCells - n1 - s;
+         uint64_t *o = a.out + (size_t)a.outRow[k] * 256;
+         const int c0 = a.complement ? 255 : 0;
+         if (n0) { atomicAdd((unsigned long long *)(o + c0), n0); }
+         if (n1) { atomicAdd((unsigned long long *)(o + (255 - c0)), n1); }
+      }
+   }
+   for (int i = threadIdx.x; i < K * 256; i += blockDim.x) {
+      const int c = i & 255;
+      const uint32_t v = sHist[i];
+      if (v && c != 0 && c != 255) {
+         const int cc = a.complement ? 255 - c : c;
+         atomicAdd((unsigned long long *)(a.out + (size_t)a.outRow[i >> 8] * 256 + cc), (unsigned long long)v);
+      }
+   }
+}
+
+// Host: the key each threshold is compared by, for "f > t" (GE false) or "f >= t" (GE true).
+// For a FP32 field the key is exact; for a FP64 field it is the high word's key (ties are
+// resolved on the device). Minus and plus zero compare equal: "> 0" uses +0's key, ">= 0" -0's.
+static uint32_t thresholdKey(double t, int enc, bool ge)
+{
+   if (t == 0.0) { t = ge ? -0.0 : 0.0; }
+   uint32_t u;
+   if (enc == ENC_F32) {
+      const float f = (float)t;  // tlo/thi are exactly representable floats here
+      memcpy(&u, &f, 4);
+   } else {
+      uint64_t b;
+      memcpy(&b, &t, 8);
+      u = (uint32_t)(b >> 32);
+   }
+   return sortKey(u);
+}
+
+template <typename T, int TY, bool GE>
+static int launchThermoT(const FusedArgs &a, cudaStream_t s)
+{
+   static int blocksPerSM = -1;
+   auto kern = thermoBPFD<T, TY, GE>;
+   const size_t stageBytes = (size_t)kThWarps * 2 * (TY + 1) * 32 * sizeof(uint32_t);
+   const size_t smem = stageBytes + (size_t)a.K * 256 * sizeof(uint32_t);
+   if (blocksPerSM < 0) {
+      const size_t maxSmem = stageBytes + (size_t)MKF_MAX_THRESH * 256 * 4;
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)maxSmem);
+      int n = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, kThWarps * 32, maxSmem);
+      blocksPerSM = n > 0 ? n : 1;
+   }
+   long long grid = (a.nItems + kThWarps - 1) / kThWarps;
+   const long long cap = (long long)smCount() * blocksPerSM;
+   if (grid > cap) { grid = cap; }
+   if (grid < 1) { grid = 1; }
+   kern<<<(unsigned)grid, kThWarps * 32, smem, s>>>(a);
+   return cudaFail(cudaGetLastError(), "thermoBPFD launch");
+}
+
+int launchThermo(FusedArgs &a, int enc, cudaStream_t s)
+{
+   const bool ge = a.rankHi != 0;
+   for (int k = 0; k < a.K; k++) { a.tkey[k] = thresholdKey(ge ? a.thi[k] : a.tlo[k], enc, ge); }
+   // the table needs at most one threshold key per bucket
+   a.lutOk = 1;
+   for (int k = 0; k + 1 < a.K; k++) {
+      if ((a.tkey[k] >> kLutShift) == (a.tkey[k + 1] >> kLutShift)) { a.lutOk = 0; }
+   }
+   if (!a.lutOk) { return MKF_ERR_UNSUPPORTED; }
+   constexpr int TY = 16;
+   a.D = 32;
+   a.nSegX = (a.X - 1 + 30) / 31;
+   a.nTileY = (a.Y - 1 + TY - 1) / TY;
+   a.nSlabZ = (a.Z - 1 + a.D - 1) / a.D;
+   a.nItems = (long long)a.nSegX * a.nTileY * a.nSlabZ;
+   if (enc == ENC_F32) { return ge ? launchThermoT<float, TY, true>(a, s) : launchThermoT<float, TY, false>(a, s); }
+   return ge ? launchThermoT<double, TY, true>(a, s) : launchThermoT<double, TY, false>(a, s);
+}
+
+}  // namespace mkf
