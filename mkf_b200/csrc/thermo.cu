@@ -23,6 +23,12 @@
 namespace mkf {
 
 static constexpr int kThWarps = 8;
+#ifndef THERMO_TY
+#define THERMO_TY 8
+#endif
+#ifndef THERMO_MINB
+#define THERMO_MINB 3
+#endif
 static constexpr int kLutShift = 18;
 static constexpr int kLutSize = 1 << (32 - kLutShift);
 
@@ -75,19 +81,32 @@ __device__ __noinline__ uint32_t exactRank(const T *__restrict__ F, long long i,
    return (v != v) ? nanRank : r;
 }
 
-// Carry-save accumulation of the 16 all-ones words of one plane (one per row pair), as a fixed
-// tree: every word enters at its row index, so no branch depends on a run-time count.
+// Carry-save accumulation of the all-ones words of one plane, one word per row pair, as a fixed
+// tree over NROW = 8 or 16 rows: every word enters at its row index (a compile-time constant in
+// the unrolled row loop), so no branch depends on a run-time count. The tree's top carries
+// (weight NROW) ripple into bit-sliced counters hi[].
+template <int NROW>
 struct PlaneOnes
 {
+   static_assert(NROW == 8 || NROW == 16, "tree of 8 or 16 rows");
    uint32_t ones = 0, twos = 0, fours = 0, eights = 0;
-   uint32_t hi[6] = {0, 0, 0, 0, 0, 0};  // sixteens, bit-sliced (up to 63 planes' worth)
+   uint32_t hi[6] = {0, 0, 0, 0, 0, 0};  // counts of NROW-weight carries (up to 63 per item)
    uint32_t p1 = 0, p2 = 0, p4 = 0, p8 = 0;
    __device__ __forceinline__ static void fa(uint32_t &s, uint32_t &c, uint32_t a, uint32_t b, uint32_t d)
    {
       s = a ^ b ^ d;
       c = (a & b) | (d & (a ^ b));
    }
-   // j is the row index 0..15; called from a fully unrolled loop, so every test on j folds away
+   __device__ __forceinline__ void ripple(uint32_t c)
+   {
+#pragma unroll
+      for (int i = 0; i < 6; i++) {
+         const uint32_t t = hi[i] & c;
+         hi[i] ^= c;
+         c = t;
+      }
+   }
+   // J is the row index; called from a fully unrolled loop, so every test on J folds away
    __device__ __forceinline__ void add(const int J, uint32_t w)
    {
       if ((J & 1) == 0) { p1 = w; return; }
@@ -97,28 +116,23 @@ struct PlaneOnes
       fa(twos, c4, twos, p2, c2);
       if ((J & 4) == 0) { p4 = c4; return; }
       fa(fours, c8, fours, p4, c4);
+      if (NROW == 8) { ripple(c8); return; }
       if ((J & 8) == 0) { p8 = c8; return; }
       fa(eights, c16, eights, p8, c8);
-#pragma unroll
-      for (int i = 0; i < 6; i++) {
-         const uint32_t t = hi[i] & c16;
-         hi[i] ^= c16;
-         c16 = t;
-      }
+      ripple(c16);
    }
    __device__ __forceinline__ uint32_t total(int k) const
    {
       uint32_t v = ((ones >> k) & 1u) + 2u * ((twos >> k) & 1u) + 4u * ((fours >> k) & 1u) + 8u * ((eights >> k) & 1u);
 #pragma unroll
-      for (int i = 0; i < 6; i++) { v += (16u << i) * ((hi[i] >> k) & 1u); }
+      for (int i = 0; i < 6; i++) { v += ((uint32_t)NROW << i) * ((hi[i] >> k) & 1u); }
       return v;
    }
 };
 
-template <typename T, int TY, bool GE>
-__global__ void __launch_bounds__(kThWarps * 32, 2) thermoBPFD(const __grid_constant__ FusedArgs a)
+template <typename T, int TY, bool GE, bool SLOT2>
+__global__ void __launch_bounds__(kThWarps * 32, TY == 8 ? THERMO_MINB : 2) thermoBPFD(const __grid_constant__ FusedArgs a)
 {
-   static_assert(TY == 16, "the all-ones tree takes 16 rows per plane");
    constexpr int W = sizeof(T) / 4;  // 32-bit words per element; the ranked word is the last one
    __shared__ uint8_t sLut[kLutSize];
    __shared__ uint32_t sKey[MKF_MAX_THRESH + 1];
@@ -184,7 +198,7 @@ __global__ void __launch_bounds__(kThWarps * 32, 2) thermoBPFD(const __grid_cons
          cpAsyncCommit();
       }
       uint32_t sF[TY], sM[TY];  // previous plane: face ranks, min | max << 8 per row pair
-      PlaneOnes ones;
+      PlaneOnes<TY> ones;
       for (int p = 0; p <= nPln; ++p) {
          P += planeStep;
          if (p < nPln) {  // stage the next plane while this one is ranked and counted
@@ -253,19 +267,38 @@ __global__ void __launch_bounds__(kThWarps * 32, 2) thermoBPFD(const __grid_cons
             const uint32_t vmask = (j < nRow) ? vx : 0u;
             const uint32_t rmax = vmask ? max(sM[j] >> 8, fmx) : rmin;  // invalid cells: no mixed codes
             ones.add(j, thermo(rmin) & vmask);
-            if (rmin < rmax) {
+            {
+               // codes of the cell for k = rmin and rmin + 1, predicated (no branch); the rare
+               // cells spanning more thresholds finish in a loop
                const uint32_t R0 = sF[j], R1 = fc;
-               uint32_t C = 0x7F7F7F7Fu - rmin * 0x01010101u;
+               const uint32_t C0 = 0x7F7F7F7Fu - rmin * 0x01010101u;
                uint32_t *h = sHist + (rmin << 8);
-               uint32_t k = rmin;
-               do {
-                  const uint32_t t0 = (R0 + C) & 0x80808080u;
-                  const uint32_t t1 = (R1 + C) & 0x80808080u;
+               {
+                  const uint32_t t0 = (R0 + C0) & 0x80808080u;
+                  const uint32_t t1 = (R1 + C0) & 0x80808080u;
                   const uint32_t c = ((t0 * 0x00204081u) >> 28) | (((t1 * 0x00204081u) >> 24) & 0xF0u);
-                  atomicAdd(h + c, 1u);
-                  C -= 0x01010101u;
-                  h += 256;
-               } while (++k < rmax);
+                  if (rmin < rmax) { atomicAdd(h + c, 1u); }
+               }
+               if (SLOT2) {
+                  const uint32_t C1 = C0 - 0x01010101u;
+                  const uint32_t t0 = (R0 + C1) & 0x80808080u;
+                  const uint32_t t1 = (R1 + C1) & 0x80808080u;
+                  const uint32_t c = ((t0 * 0x00204081u) >> 28) | (((t1 * 0x00204081u) >> 24) & 0xF0u);
+                  if (rmin + 1 < rmax) { atomicAdd(h + 256 + c, 1u); }
+                  if (rmin + 2 < rmax) {
+                     uint32_t C = C1 - 0x01010101u;
+                     uint32_t *hk = h + 512;
+                     uint32_t k = rmin + 2;
+                     do {
+                        const uint32_t u0 = (R0 + C) & 0x80808080u;
+                        const uint32_t u1 = (R1 + C) & 0x80808080u;
+                        const uint32_t cc = ((u0 * 0x00204081u) >> 28) | (((u1 * 0x00204081u) >> 24) & 0xF0u);
+                        atomicAdd(hk + cc, 1u);
+                        C -= 0x01010101u;
+                        hk += 256;
+                     } while (++k < rmax);
+                  }
+               }
             }
             sF[j] = fc;
             sM[j] = fmn | (fmx << 8);
@@ -324,11 +357,11 @@ static uint32_t thresholdKey(double t, int enc, bool ge)
    return sortKey(u);
 }
 
-template <typename T, int TY, bool GE>
+template <typename T, int TY, bool GE, bool SLOT2>
 static int launchThermoT(const FusedArgs &a, cudaStream_t s)
 {
    static int blocksPerSM = -1;
-   auto kern = thermoBPFD<T, TY, GE>;
+   auto kern = thermoBPFD<T, TY, GE, SLOT2>;
    const size_t stageBytes = (size_t)kThWarps * 2 * (TY + 1) * 32 * sizeof(uint32_t);
    const size_t smem = stageBytes + (size_t)a.K * 256 * sizeof(uint32_t);
    if (blocksPerSM < 0) {
@@ -356,14 +389,19 @@ int launchThermo(FusedArgs &a, int enc, cudaStream_t s)
       if ((a.tkey[k] >> kLutShift) == (a.tkey[k + 1] >> kLutShift)) { a.lutOk = 0; }
    }
    if (!a.lutOk) { return MKF_ERR_UNSUPPORTED; }
-   constexpr int TY = 16;
+   constexpr int TY = THERMO_TY;
    a.D = 32;
    a.nSegX = (a.X - 1 + 30) / 31;
    a.nTileY = (a.Y - 1 + TY - 1) / TY;
    a.nSlabZ = (a.Z - 1 + a.D - 1) / a.D;
    a.nItems = (long long)a.nSegX * a.nTileY * a.nSlabZ;
-   if (enc == ENC_F32) { return ge ? launchThermoT<float, TY, true>(a, s) : launchThermoT<float, TY, false>(a, s); }
-   return ge ? launchThermoT<double, TY, true>(a, s) : launchThermoT<double, TY, false>(a, s);
+   // one threshold: a cell has at most one mixed code
+   if (a.K == 1) {
+      if (enc == ENC_F32) { return ge ? launchThermoT<float, TY, true, false>(a, s) : launchThermoT<float, TY, false, false>(a, s); }
+      return ge ? launchThermoT<double, TY, true, false>(a, s) : launchThermoT<double, TY, false, false>(a, s);
+   }
+   if (enc == ENC_F32) { return ge ? launchThermoT<float, TY, true, true>(a, s) : launchThermoT<float, TY, false, true>(a, s); }
+   return ge ? launchThermoT<double, TY, true, true>(a, s) : launchThermoT<double, TY, false, true>(a, s);
 }
 
 }  // namespace mkf
