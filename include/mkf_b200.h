@@ -94,8 +94,20 @@ int mkfFieldBPFDHost(uint64_t *pBPFDH, const MKFFieldDesc *pF, const MKFThreshSe
 int mkfFieldBPFDHostNoAlloc(uint64_t *pBPFDH, const MKFFieldDesc *pF, const MKFThreshSet *pT, void *stream);
 
 /* ---- many fields, one launch (no original counterpart; the original runs one field per call) ---- */
-/* Fields i = 0..nF-1 (device pointers) with threshold sets pT[i]; the counts of field i start at
- * pBPFD + 256 * (nT_0 + ... + nT_{i-1}). */
+/* Fields i = 0..nF-1 (device pointers, any shapes, FP32/FP64) with threshold sets pT[i]; the counts
+ * of field i are rows nT_0 + ... + nT_{i-1} onwards of pBPFD (device, overwritten). One persistent
+ * launch walks a work list of (field, item chunk) entries; fields whose thresholds mix relations
+ * are counted by their own pass. A plan keeps the work list on the device so the same batch (same
+ * buffers, new contents) can be launched again, also inside a CUDA graph. */
+typedef struct MKFBatchPlan MKFBatchPlan;
+int mkfBatchPlanCreate(MKFBatchPlan **pPlan, uint64_t *pBPFD, const MKFFieldDesc *pF, const MKFThreshSet *pT, int nF);
+/* Clear the counts and count every field, asynchronously on `stream`; issues no allocation and no
+ * synchronisation, so it may be captured into a CUDA graph. */
+int mkfBatchPlanLaunch(MKFBatchPlan *plan, void *stream);
+/* The same through a CUDA graph the plan captures on first use and replays afterwards. */
+int mkfBatchPlanLaunchGraph(MKFBatchPlan *plan, void *stream);
+int mkfBatchPlanDestroy(MKFBatchPlan *plan);
+/* One-shot: create a plan, launch it on `stream`, wait for it and destroy it (synchronous). */
 int mkfBatchBPFD(uint64_t *pBPFD, const MKFFieldDesc *pF, const MKFThreshSet *pT, int nF, int flags, void *stream);
 
 /* ---- measures (closest original: mkfSelectMeasuresBPFD, mkfUtil.c:94) ---- */

@@ -19,7 +19,7 @@ from ._lib import (BMC_AL, BMC_EQ, BMC_GT, BMC_LT, ENC_F32, ENC_F64, MKF_F_ACCUM
                    BMOrg, ConstFieldPtr, KernInfo, MKFError, MKFFieldDesc, MKFThreshSet, check, lib)
 
 __all__ = [
-    "build", "lib", "MKFError", "relation_mask", "field_bpfd", "field_bpfd_host", "batch_bpfd",
+    "build", "lib", "MKFError", "BatchPlan", "relation_mask", "field_bpfd", "field_bpfd_host", "batch_bpfd",
     "bin_map_cuda", "get_bpfd", "get_bpfd_host", "measures", "measures_dev", "select_measures",
     "ENC_F32", "ENC_F64", "BMC_LT", "BMC_EQ", "BMC_GT", "BMC_AL",
 ]
@@ -148,6 +148,50 @@ def batch_bpfd(fields, thresholds_list, masks=None, out=None, stream=None):
     rc = lib().mkfBatchBPFD(out.data_ptr(), descs, sets, n, 0, _stream_ptr(stream))
     check(rc, "mkfBatchBPFD")
     return out
+
+
+class BatchPlan:
+    """A reusable batch (mkfBatchPlanCreate): the work list stays on the device, so the same fields
+    (same buffers, new contents) can be counted again with launch() or as a CUDA graph with
+    launch_graph()."""
+
+    def __init__(self, fields, thresholds_list, masks=None, out=None):
+        torch = _torch()
+        n = len(fields)
+        masks = masks if masks is not None else [BMC_GT] * n
+        self._ths = [_Thresholds(t, m) for t, m in zip(thresholds_list, masks)]
+        total = sum(t.n for t in self._ths)
+        self.out = out if out is not None else torch.zeros((total, 256), dtype=torch.int64, device=fields[0].device)
+        self._fields = list(fields)
+        descs = (MKFFieldDesc * n)()
+        sets = (MKFThreshSet * n)()
+        for i, f in enumerate(fields):
+            strides = None if f.is_contiguous() else f.stride()
+            descs[i] = _field_desc(f.data_ptr(), _enc_of(f), f.shape, strides)
+            sets[i] = self._ths[i].ts
+        h = C.c_void_p()
+        check(lib().mkfBatchPlanCreate(C.byref(h), self.out.data_ptr(), descs, sets, n), "mkfBatchPlanCreate")
+        self._h = h
+
+    def launch(self, stream=None):
+        check(lib().mkfBatchPlanLaunch(self._h, _stream_ptr(stream)), "mkfBatchPlanLaunch")
+        return self.out
+
+    def launch_graph(self, stream=None):
+        check(lib().mkfBatchPlanLaunchGraph(self._h, _stream_ptr(stream)), "mkfBatchPlanLaunchGraph")
+        return self.out
+
+    def close(self):
+        if self._h:
+            _torch().cuda.synchronize()
+            lib().mkfBatchPlanDestroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def bin_map_cuda(fields, rel: str, t: float, prof_id: int = 0, out=None, strides_zyx=None):

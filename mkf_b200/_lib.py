@@ -104,6 +104,10 @@ _SIG = [
     ("mkfFieldBPFD", C.c_int, [_P, C.POINTER(MKFFieldDesc), C.POINTER(MKFThreshSet), C.c_int, _P]),
     ("mkfFieldBPFDHost", C.c_int, [_P, C.POINTER(MKFFieldDesc), C.POINTER(MKFThreshSet)]),
     ("mkfFieldBPFDHostNoAlloc", C.c_int, [_P, C.POINTER(MKFFieldDesc), C.POINTER(MKFThreshSet), _P]),
+    ("mkfBatchPlanCreate", C.c_int, [C.POINTER(C.c_void_p), _P, C.POINTER(MKFFieldDesc), C.POINTER(MKFThreshSet), C.c_int]),
+    ("mkfBatchPlanLaunch", C.c_int, [_P, _P]),
+    ("mkfBatchPlanLaunchGraph", C.c_int, [_P, _P]),
+    ("mkfBatchPlanDestroy", C.c_int, [_P]),
     ("mkfBatchBPFD", C.c_int, [_P, C.POINTER(MKFFieldDesc), C.POINTER(MKFThreshSet), C.c_int, C.c_int, _P]),
     ("mkfMeasuresF64", C.c_int, [_P, _P, C.c_int]),
     ("mkfMeasuresF64Dev", C.c_int, [_P, _P, C.c_int, _P]),

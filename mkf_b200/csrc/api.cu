@@ -3,7 +3,7 @@
 #include <cstring>
 #include <mutex>
 #include <vector>
-#include "mkf_common.cuh"
+#include "fused.cuh"
 
 namespace mkf {
 int fieldBPFD(uint64_t *out, const MKFFieldDesc *pF, const MKFThreshSet *pT, int flags, cudaStream_t s, const int *rowBase);
@@ -83,16 +83,185 @@ MKF_API int mkfFieldBPFD(uint64_t *pBPFD, const MKFFieldDesc *pF, const MKFThres
    return fieldBPFD(pBPFD, pF, pT, flags, (cudaStream_t)stream, nullptr);
 }
 
-MKF_API int mkfBatchBPFD(uint64_t *pBPFD, const MKFFieldDesc *pF, const MKFThreshSet *pT, int nF, int flags, void *stream)
+// ---------------------------------------------------------------- batches
+
+struct MKFBatchPlan
 {
-   if (!pBPFD || !pF || !pT || nF < 0) { setError("mkfBatchBPFD: bad argument"); return MKF_ERR_ARG; }
+   uint64_t *out = nullptr;
+   size_t rows = 0;
+   FieldTask *dTasks = nullptr;
+   BatchChunk *dChunks = nullptr;
+   unsigned *dCounter = nullptr;
+   int nChunks = 0;
+   std::vector<ConstEntry> consts;
+   std::vector<unsigned long long> constCells;
+   struct Fallback
+   {
+      MKFFieldDesc d;
+      std::vector<double> t;
+      std::vector<uint32_t> m;
+      uint32_t mAll;
+      bool perThreshold;
+      size_t rowBase;
+   };
+   std::vector<Fallback> fallbacks;
+   cudaGraph_t graph = nullptr;
+   cudaGraphExec_t graphExec = nullptr;
+};
+
+static constexpr int kChunkItems = 64;
+
+static void freePlan(MKFBatchPlan *p)
+{
+   if (!p) { return; }
+   if (p->graphExec) { cudaGraphExecDestroy(p->graphExec); }
+   if (p->graph) { cudaGraphDestroy(p->graph); }
+   if (p->dTasks) { cudaFree(p->dTasks); }
+   if (p->dChunks) { cudaFree(p->dChunks); }
+   if (p->dCounter) { cudaFree(p->dCounter); }
+   delete p;
+}
+
+MKF_API int mkfBatchPlanCreate(MKFBatchPlan **pp, uint64_t *pBPFD, const MKFFieldDesc *pF, const MKFThreshSet *pT, int nF)
+{
+   if (!pp || !pBPFD || (nF > 0 && (!pF || !pT)) || nF < 0) { setError("mkfBatchPlanCreate: bad argument"); return MKF_ERR_ARG; }
+   *pp = nullptr;
+   MKFBatchPlan *p = new MKFBatchPlan();
+   p->out = pBPFD;
+   std::vector<FieldTask> tasks;
+   std::vector<BatchChunk> chunks;
    size_t row = 0;
    for (int i = 0; i < nF; i++) {
-      const int rc = fieldBPFD(pBPFD + row * 256, pF + i, pT + i, flags, (cudaStream_t)stream, nullptr);
-      if (rc != MKF_OK) { return rc; }
-      row += (size_t)pT[i].nT;
+      const MKFFieldDesc *d = pF + i;
+      const MKFThreshSet *ts = pT + i;
+      if (!d->p || !ts->t || ts->nT < 1 || ts->nT > MKF_MAX_THRESH || (d->enc != ENC_F32 && d->enc != ENC_F64) ||
+          d->def[0] < 1 || d->def[1] < 1 || d->def[2] < 1) {
+         setError("mkfBatchPlanCreate: field %d: bad descriptor or thresholds", i);
+         freePlan(p);
+         return MKF_ERR_ARG;
+      }
+      const unsigned long long cells = (unsigned long long)(d->def[0] - 1) * (d->def[1] - 1) * (d->def[2] - 1);
+      const size_t c0 = p->consts.size();
+      FieldTask t;
+      bool varying = false;
+      const bool ok = planBatchField(d, ts, (int)row, t, p->consts, varying);
+      for (size_t c = c0; c < p->consts.size(); c++) { p->constCells.push_back(cells); }
+      if (cells > 0 && ok) {
+         const int f = (int)tasks.size();
+         for (long long b = 0; b < t.nItems; b += kChunkItems) {
+            chunks.push_back({f, 0, b, std::min<long long>(b + kChunkItems, t.nItems)});
+         }
+         t.out = pBPFD;
+         tasks.push_back(t);
+      } else if (cells > 0 && varying) {
+         MKFBatchPlan::Fallback fb;
+         fb.d = *d;
+         fb.t.assign(ts->t, ts->t + ts->nT);
+         fb.perThreshold = ts->m != nullptr;
+         if (fb.perThreshold) { fb.m.assign(ts->m, ts->m + ts->nT); }
+         fb.mAll = ts->mAll;
+         fb.rowBase = row;
+         // constant maps of this field are counted by its own pass
+         p->consts.resize(c0);
+         p->constCells.resize(c0);
+         p->fallbacks.push_back(fb);
+      }
+      row += (size_t)ts->nT;
    }
+   p->rows = row;
+   cudaError_t e = cudaSuccess;
+   if (!tasks.empty()) {
+      e = cudaMalloc(&p->dTasks, tasks.size() * sizeof(FieldTask));
+      if (e == cudaSuccess) { e = cudaMalloc(&p->dChunks, chunks.size() * sizeof(BatchChunk)); }
+      if (e == cudaSuccess) { e = cudaMalloc(&p->dCounter, sizeof(unsigned)); }
+      if (e == cudaSuccess) { e = cudaMemcpy(p->dTasks, tasks.data(), tasks.size() * sizeof(FieldTask), cudaMemcpyHostToDevice); }
+      if (e == cudaSuccess) { e = cudaMemcpy(p->dChunks, chunks.data(), chunks.size() * sizeof(BatchChunk), cudaMemcpyHostToDevice); }
+      p->nChunks = (int)chunks.size();
+   }
+   if (e != cudaSuccess) {
+      freePlan(p);
+      return cudaFail(e, "mkfBatchPlanCreate: device work list");
+   }
+   *pp = p;
    return MKF_OK;
+}
+
+// Everything a launch issues, in stream order (no allocation, no synchronisation: capturable).
+static int planLaunchOn(MKFBatchPlan *p, cudaStream_t s)
+{
+   cudaError_t e = cudaMemsetAsync(p->out, 0, p->rows * 256 * sizeof(uint64_t), s);
+   if (e != cudaSuccess) { return cudaFail(e, "batch output clear"); }
+   int rc = MKF_OK;
+   for (size_t i = 0; i < p->consts.size() && rc == MKF_OK; i++) {
+      rc = launchConstBin(p->out, p->consts[i].row, p->consts[i].bin, p->constCells[i], s);
+   }
+   if (rc == MKF_OK && p->nChunks > 0) {
+      e = cudaMemsetAsync(p->dCounter, 0, sizeof(unsigned), s);
+      if (e != cudaSuccess) { return cudaFail(e, "batch counter clear"); }
+      BatchArgs b;
+      b.tasks = p->dTasks;
+      b.chunks = p->dChunks;
+      b.nChunks = p->nChunks;
+      b.counter = p->dCounter;
+      rc = launchThermoBatch(b, s);
+   }
+   for (size_t i = 0; i < p->fallbacks.size() && rc == MKF_OK; i++) {
+      const MKFBatchPlan::Fallback &fb = p->fallbacks[i];
+      MKFThreshSet ts;
+      ts.nT = (int32_t)fb.t.size();
+      ts.t = fb.t.data();
+      ts.m = fb.perThreshold ? fb.m.data() : nullptr;
+      ts.mAll = fb.mAll;
+      rc = fieldBPFD(p->out + fb.rowBase * 256, &fb.d, &ts, MKF_F_ACCUMULATE, s, nullptr);
+   }
+   return rc;
+}
+
+MKF_API int mkfBatchPlanLaunch(MKFBatchPlan *p, void *stream)
+{
+   if (!p) { setError("mkfBatchPlanLaunch: NULL plan"); return MKF_ERR_ARG; }
+   return planLaunchOn(p, (cudaStream_t)stream);
+}
+
+MKF_API int mkfBatchPlanLaunchGraph(MKFBatchPlan *p, void *stream)
+{
+   if (!p) { setError("mkfBatchPlanLaunchGraph: NULL plan"); return MKF_ERR_ARG; }
+   cudaError_t e;
+   if (!p->graphExec) {
+      cudaStream_t cap;
+      e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
+      if (e != cudaSuccess) { return cudaFail(e, "capture stream"); }
+      e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+      int rc = (e == cudaSuccess) ? planLaunchOn(p, cap) : cudaFail(e, "cudaStreamBeginCapture");
+      cudaGraph_t g = nullptr;
+      e = cudaStreamEndCapture(cap, &g);
+      cudaStreamDestroy(cap);
+      if (rc != MKF_OK) { if (g) { cudaGraphDestroy(g); } return rc; }
+      if (e != cudaSuccess) { return cudaFail(e, "cudaStreamEndCapture"); }
+      e = cudaGraphInstantiate(&p->graphExec, g, 0);
+      if (e != cudaSuccess) { cudaGraphDestroy(g); return cudaFail(e, "cudaGraphInstantiate"); }
+      p->graph = g;
+   }
+   return cudaFail(cudaGraphLaunch(p->graphExec, (cudaStream_t)stream), "cudaGraphLaunch");
+}
+
+MKF_API int mkfBatchPlanDestroy(MKFBatchPlan *p)
+{
+   freePlan(p);
+   return MKF_OK;
+}
+
+MKF_API int mkfBatchBPFD(uint64_t *pBPFD, const MKFFieldDesc *pF, const MKFThreshSet *pT, int nF, int flags, void *stream)
+{
+   (void)flags;
+   MKFBatchPlan *p = nullptr;
+   int rc = mkfBatchPlanCreate(&p, pBPFD, pF, pT, nF);
+   if (rc != MKF_OK) { return rc; }
+   rc = planLaunchOn(p, (cudaStream_t)stream);
+   const cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+   if (rc == MKF_OK) { rc = cudaFail(e, "batch synchronisation"); }
+   freePlan(p);
+   return rc;
 }
 
 MKF_API int mkfMeasuresF64Dev(double *r, const uint64_t *pBPFD, int nSets, void *stream)

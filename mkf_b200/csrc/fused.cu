@@ -234,8 +234,6 @@ __global__ void addConstBin(uint64_t *out, int row, int bin, unsigned long long 
 
 // ------------------------------------------------------------------ host side
 
-struct ConstEntry { int row, bin; };
-
 struct Pass
 {
    bool thermo;
@@ -335,6 +333,57 @@ int launchConstBin(uint64_t *out, int row, int bin, unsigned long long cells, cu
 }
 
 void floatBoundsPlain(double t, double &tlo, double &thi) { floatBounds(t, tlo, thi); }
+
+// Split one field of a batch: constant maps go to `consts` (rows offset by rowBase); if every other
+// threshold shares one thermometer relation and the thresholds fit the rank table, `t` is filled
+// for the batched kernel and true is returned; otherwise the field takes the single-field path.
+bool planBatchField(const MKFFieldDesc *pF, const MKFThreshSet *pT, int rowBase, FieldTask &t, std::vector<ConstEntry> &consts,
+                    bool &anyVarying)
+{
+   memset(&t, 0, sizeof(t));
+   const int K = pT->nT;
+   int idx[MKF_MAX_THRESH], n = 0, cls0 = -2;
+   for (int i = 0; i < K; i++) {
+      const double tv = pT->t[i];
+      const uint32_t m = (pT->m ? pT->m[i] : pT->mAll) & BMC_AL;
+      if (m == 0 || m == BMC_AL || std::isnan(tv)) {
+         const bool one = (m == BMC_AL) || (std::isnan(tv) && (m & BMC_EQ));
+         consts.push_back({rowBase + i, one ? 255 : 0});
+         continue;
+      }
+      int cls = -1;
+      if (m == BMC_GT) { cls = 0; }
+      else if (m == (BMC_GT | BMC_EQ)) { cls = 1; }
+      else if (m == BMC_LT) { cls = 2; }
+      else if (m == (BMC_LT | BMC_EQ)) { cls = 3; }
+      if (n == 0) { cls0 = cls; }
+      else if (cls != cls0) { cls0 = -1; }
+      idx[n++] = i;
+   }
+   anyVarying = n > 0;
+   if (n == 0 || cls0 < 0) { return false; }
+   std::stable_sort(idx, idx + n, [&](int x, int y) { return pT->t[x] < pT->t[y]; });
+   const int X = pF->def[0], Y = pF->def[1], Z = pF->def[2];
+   const bool planar = !(pF->stride[0] | pF->stride[1] | pF->stride[2]);
+   t.f = pF->p;
+   t.sx = planar ? 1 : pF->stride[0];
+   t.sy = planar ? (int64_t)X : pF->stride[1];
+   t.sz = planar ? (int64_t)X * Y : pF->stride[2];
+   t.X = X; t.Y = Y; t.Z = Z;
+   t.K = n;
+   for (int i = 0; i < 64; i++) { t.tlo[i] = INFINITY; t.thi[i] = INFINITY; }
+   for (int k = 0; k < n; k++) {
+      const double tv = pT->t[idx[k]];
+      if (pF->enc == ENC_F32) { floatBounds(tv, t.tlo[k], t.thi[k]); }
+      else { t.tlo[k] = t.thi[k] = tv; }
+      t.outRow[k] = rowBase + idx[k];
+   }
+   t.rankHi = (cls0 == 1 || cls0 == 2);
+   t.complement = (cls0 >= 2);
+   const bool eqBit = (cls0 == 1 || cls0 == 3);
+   t.nanRank = (eqBit != (t.complement != 0)) ? (uint32_t)n : 0u;
+   return prepareThermoTask(t, pF->enc);
+}
 
 int fieldBPFD(uint64_t *out, const MKFFieldDesc *pF, const MKFThreshSet *pT, int flags, cudaStream_t s,
               const int *rowBase /* output row of threshold i, NULL = identity */)

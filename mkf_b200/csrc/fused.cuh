@@ -1,5 +1,6 @@
 // fused.cuh - arguments shared by the fused counting kernels (fused.cu, thermo.cu).
 #pragma once
+#include <vector>
 #include "mkf_common.cuh"
 
 namespace mkf {
@@ -27,6 +28,44 @@ struct FusedArgs
    int lutOk;
 };
 
+
+// One field of a batch, as the batched thermometer kernel reads it from device memory.
+struct FieldTask
+{
+   const void *f;
+   int64_t sx, sy, sz;
+   int X, Y, Z, K, D, nSegX, nTileY, nSlabZ;
+   long long nItems;
+   uint32_t nanRank;
+   int rankHi, complement, variant;  // variant: 0 f32 >, 1 f32 >=, 2 f64 >, 3 f64 >=
+   uint64_t *out;
+   int outRow[MKF_MAX_THRESH];
+   uint32_t tkey[MKF_MAX_THRESH];
+   double tlo[64], thi[64];
+};
+
+// Consecutive work items [begin, end) of one field.
+struct BatchChunk
+{
+   int field, pad_;
+   long long begin, end;
+};
+
+struct BatchArgs
+{
+   const FieldTask *tasks;
+   const BatchChunk *chunks;
+   int nChunks;
+   unsigned *counter;  // next chunk to hand out; zero at launch
+};
+
+struct ConstEntry { int row, bin; };
+bool planBatchField(const MKFFieldDesc *pF, const MKFThreshSet *pT, int rowBase, FieldTask &t, std::vector<ConstEntry> &consts,
+                    bool &anyVarying);
+
+// Fill a task's key table and item grid; false if its thresholds share a rank-table bucket.
+bool prepareThermoTask(FieldTask &t, int enc);
+int launchThermoBatch(const BatchArgs &b, cudaStream_t s);
 
 // Launch the thermometer kernel for a pass whose thresholds all share one relation
 // (< <= > >=); fills the key table of `a` first.

@@ -65,8 +65,8 @@ __device__ __forceinline__ void cpAsyncWait() { asm volatile("cp.async.wait_grou
 // Exact rank of the element F[i] by binary search over the sorted thresholds in the field's
 // precision. Kept out of line: it runs only for the rare elements the fast path cannot decide.
 template <typename T, bool GE>
-__device__ __noinline__ uint32_t exactRank(const T *__restrict__ F, long long i, const T *sTlo, const T *sThi, int K,
-                                           uint32_t nanRank)
+__device__ __noinline__ uint32_t exactRank(const T *__restrict__ F, long long i, const double *sTlo, const double *sThi,
+                                           int K, uint32_t nanRank)
 {
    const T v = __ldg(F + i);
    uint32_t r = 0;
@@ -130,199 +130,62 @@ struct PlaneOnes
    }
 };
 
-template <typename T, int TY, bool GE, bool SLOT2>
-__global__ void __launch_bounds__(kThWarps * 32, TY == 8 ? THERMO_MINB : 2) thermoBPFD(const __grid_constant__ FusedArgs a)
+// Shared state of a CTA while it counts one field: the rank table, the thresholds, and the
+// per-threshold totals. The [K][256] histogram and the warps' staging planes are dynamic.
+struct ThermoShared
 {
-   constexpr int W = sizeof(T) / 4;  // 32-bit words per element; the ranked word is the last one
-   __shared__ uint8_t sLut[kLutSize];
-   __shared__ uint32_t sKey[MKF_MAX_THRESH + 1];
-   __shared__ T sTlo[64];
-   __shared__ T sThi[64];
-   __shared__ uint32_t sOnes[MKF_MAX_THRESH];
-   __shared__ unsigned long long sCells;
-   // dynamic shared memory: per warp, two planes of the 32-bit words each lane ranks
-   // ([warp][buffer][row][lane]), then the [K][256] histogram
-   extern __shared__ uint32_t sDyn[];
-   uint32_t *sHist = sDyn + kThWarps * 2 * (TY + 1) * 32;
+   uint8_t lut[kLutSize];
+   uint32_t key[MKF_MAX_THRESH + 1];
+   double tlo[64];
+   double thi[64];
+   uint32_t ones[MKF_MAX_THRESH];
+   unsigned long long cells;
+};
 
+template <int TY>
+__device__ __forceinline__ uint32_t *histOf(uint32_t *dyn) { return dyn + kThWarps * 2 * (TY + 1) * 32; }
+
+// Load one field's thresholds, build its rank table and clear the histogram (whole CTA).
+template <int TY, typename P>
+__device__ void ctaSetup(const P &a, ThermoShared &S, uint32_t *dyn)
+{
    const int K = a.K;
-   for (int i = threadIdx.x; i < K * 256; i += blockDim.x) { sHist[i] = 0; }
+   uint32_t *hist = histOf<TY>(dyn);
+   for (int i = threadIdx.x; i < K * 256; i += blockDim.x) { hist[i] = 0; }
    for (int i = threadIdx.x; i < 64; i += blockDim.x) {
-      sTlo[i] = (T)a.tlo[i];
-      sThi[i] = (T)a.thi[i];
+      S.tlo[i] = a.tlo[i];
+      S.thi[i] = a.thi[i];
    }
-   for (int i = threadIdx.x; i <= MKF_MAX_THRESH; i += blockDim.x) { sKey[i] = (i < K) ? a.tkey[i] : 0xFFFFFFFFu; }
+   for (int i = threadIdx.x; i <= MKF_MAX_THRESH; i += blockDim.x) { S.key[i] = (i < K) ? a.tkey[i] : 0xFFFFFFFFu; }
+   __syncthreads();
    // bucket b -> number of threshold keys below the bucket's first key
    for (int b = threadIdx.x; b < kLutSize; b += blockDim.x) {
       const uint32_t start = (uint32_t)b << kLutShift;
       uint32_t n = 0;
-      for (int k = 0; k < K; k++) { n += a.tkey[k] < start; }
-      sLut[b] = (uint8_t)n;
+      for (int k = 0; k < K; k++) { n += S.key[k] < start; }
+      S.lut[b] = (uint8_t)n;
    }
-   if (threadIdx.x < MKF_MAX_THRESH) { sOnes[threadIdx.x] = 0; }
-   if (threadIdx.x == 0) { sCells = 0; }
+   if (threadIdx.x < MKF_MAX_THRESH) { S.ones[threadIdx.x] = 0; }
+   if (threadIdx.x == 0) { S.cells = 0; }
    __syncthreads();
+}
 
-   const int lane = threadIdx.x & 31;
-   uint32_t(*stage)[TY + 1][32] = reinterpret_cast<uint32_t(*)[TY + 1][32]>(sDyn + (threadIdx.x >> 5) * 2 * (TY + 1) * 32);
-   const long long gw = (long long)blockIdx.x * kThWarps + (threadIdx.x >> 5);
-   const long long nw = (long long)gridDim.x * kThWarps;
-   const unsigned *__restrict__ F32w = reinterpret_cast<const unsigned *>(a.f) + (W - 1);
-   const long long rowStep = (long long)W * a.sy, planeStep = (long long)W * a.sz;
-   const uint32_t nanRank = a.nanRank;
-   unsigned long long cells = 0;
-
-   for (long long it = gw; it < a.nItems; it += nw) {
-      const int ix = (int)(it % a.nSegX);
-      const long long rest = it / a.nSegX;
-      const int iy = (int)(rest % a.nTileY);
-      const int iz = (int)(rest / a.nTileY);
-      const int x0 = 31 * ix, y0 = TY * iy, z0 = a.D * iz;
-      const int xl = min(x0 + lane, a.X - 1);  // lanes past the row end re-read the last element
-      const uint32_t vx = ((lane < 31) && (x0 + lane < a.X - 1)) ? 0xFFFFFFFFu : 0u;
-      const int nRow = min(TY, a.Y - 1 - y0);
-      const int nPln = min(a.D, a.Z - 1 - z0);
-      cells += (unsigned long long)max(0, min(31, a.X - 1 - x0)) * (unsigned)nRow * (unsigned)nPln;
-      const int lastRow = a.Y - 1 - y0;  // rows j > lastRow re-read row lastRow
-      // word offsets of the TY+1 rows relative to the row y0 (clamped), kept as 32-bit steps
-      const unsigned *__restrict__ P = F32w + (long long)W * ((long long)xl * a.sx + (long long)y0 * a.sy + (long long)z0 * a.sz);
-
-      // stage plane 0; every lane later reads back only the words it copied itself
-      {
-         const unsigned *q = P;
-#pragma unroll
-         for (int j = 0; j <= TY; ++j) {
-            cpAsync4(&stage[0][j][lane], q);
-            if (j < lastRow) { q += rowStep; }
-         }
-         cpAsyncCommit();
-      }
-      uint32_t sF[TY], sM[TY];  // previous plane: face ranks, min | max << 8 per row pair
-      PlaneOnes<TY> ones;
-      for (int p = 0; p <= nPln; ++p) {
-         P += planeStep;
-         if (p < nPln) {  // stage the next plane while this one is ranked and counted
-            const unsigned *q = P;
-#pragma unroll
-            for (int j = 0; j <= TY; ++j) {
-               cpAsync4(&stage[(p + 1) & 1][j][lane], q);
-               if (j < lastRow) { q += rowStep; }
-            }
-            cpAsyncCommit();
-            cpAsyncWait<1>();
-         } else {
-            cpAsyncWait<0>();
-         }
-         const uint32_t(*w)[32] = stage[p & 1];
-         uint32_t r[TY + 1];
-         uint32_t slow = 0;  // bit j: element of row j needs the exact rank
-#pragma unroll
-         for (int j = 0; j <= TY; ++j) {
-            const uint32_t wj = w[j][lane];
-            const uint32_t key = sortKey(wj);
-            const uint32_t r0 = sLut[key >> kLutShift];
-            const uint32_t cand = sKey[r0];
-            r[j] = r0 + (GE ? (key >= cand) : (key > cand));
-            if (W == 2) {
-               slow |= (uint32_t)((key == cand) | ((key - 0x00100000u) >= 0xFFE00000u)) << j;
-            } else {
-               r[j] = ((wj & 0x7FFFFFFFu) > 0x7F800000u) ? nanRank : r[j];
-            }
-         }
-         if (W == 2 && slow) {
-            const T *Fe = reinterpret_cast<const T *>(a.f);
-            const long long e0 = (long long)xl * a.sx + (long long)y0 * a.sy + (long long)(z0 + p) * a.sz;
-#pragma unroll
-            for (int j = 0; j <= TY; ++j) {
-               if ((slow >> j) & 1u) {
-                  r[j] = exactRank<T, GE>(Fe, e0 + (long long)min(j, lastRow) * a.sy, sTlo, sThi, K, nanRank);
-               }
-            }
-         }
-         uint32_t rR = __shfl_down_sync(FULL, r[0], 1);
-         uint32_t ePrev = __byte_perm(r[0], rR, 0x0040);
-         uint32_t mnPrev = min(r[0], rR), mxPrev = max(r[0], rR);
-         if (p == 0) {
-#pragma unroll
-            for (int j = 0; j < TY; ++j) {
-               rR = __shfl_down_sync(FULL, r[j + 1], 1);
-               const uint32_t e = __byte_perm(r[j + 1], rR, 0x0040);
-               const uint32_t mn = min(r[j + 1], rR), mx = max(r[j + 1], rR);
-               sF[j] = __byte_perm(ePrev, e, 0x5410);
-               sM[j] = min(mnPrev, mn) | (max(mxPrev, mx) << 8);
-               ePrev = e;
-               mnPrev = mn;
-               mxPrev = mx;
-            }
-            continue;
-         }
-#pragma unroll
-         for (int j = 0; j < TY; ++j) {
-            rR = __shfl_down_sync(FULL, r[j + 1], 1);
-            const uint32_t e = __byte_perm(r[j + 1], rR, 0x0040);
-            const uint32_t mn = min(r[j + 1], rR), mx = max(r[j + 1], rR);
-            const uint32_t fc = __byte_perm(ePrev, e, 0x5410);
-            const uint32_t fmn = min(mnPrev, mn), fmx = max(mxPrev, mx);
-            const uint32_t rmin = min(sM[j] & 0xFFu, fmn);
-            const uint32_t vmask = (j < nRow) ? vx : 0u;
-            const uint32_t rmax = vmask ? max(sM[j] >> 8, fmx) : rmin;  // invalid cells: no mixed codes
-            ones.add(j, thermo(rmin) & vmask);
-            {
-               // codes of the cell for k = rmin and rmin + 1, predicated (no branch); the rare
-               // cells spanning more thresholds finish in a loop
-               const uint32_t R0 = sF[j], R1 = fc;
-               const uint32_t C0 = 0x7F7F7F7Fu - rmin * 0x01010101u;
-               uint32_t *h = sHist + (rmin << 8);
-               {
-                  const uint32_t t0 = (R0 + C0) & 0x80808080u;
-                  const uint32_t t1 = (R1 + C0) & 0x80808080u;
-                  const uint32_t c = ((t0 * 0x00204081u) >> 28) | (((t1 * 0x00204081u) >> 24) & 0xF0u);
-                  if (rmin < rmax) { atomicAdd(h + c, 1u); }
-               }
-               if (SLOT2) {
-                  const uint32_t C1 = C0 - 0x01010101u;
-                  const uint32_t t0 = (R0 + C1) & 0x80808080u;
-                  const uint32_t t1 = (R1 + C1) & 0x80808080u;
-                  const uint32_t c = ((t0 * 0x00204081u) >> 28) | (((t1 * 0x00204081u) >> 24) & 0xF0u);
-                  if (rmin + 1 < rmax) { atomicAdd(h + 256 + c, 1u); }
-                  if (rmin + 2 < rmax) {
-                     uint32_t C = C1 - 0x01010101u;
-                     uint32_t *hk = h + 512;
-                     uint32_t k = rmin + 2;
-                     do {
-                        const uint32_t u0 = (R0 + C) & 0x80808080u;
-                        const uint32_t u1 = (R1 + C) & 0x80808080u;
-                        const uint32_t cc = ((u0 * 0x00204081u) >> 28) | (((u1 * 0x00204081u) >> 24) & 0xF0u);
-                        atomicAdd(hk + cc, 1u);
-                        C -= 0x01010101u;
-                        hk += 256;
-                     } while (++k < rmax);
-                  }
-               }
-            }
-            sF[j] = fc;
-            sM[j] = fmn | (fmx << 8);
-            ePrev = e;
-            mnPrev = mn;
-            mxPrev = mx;
-         }
-      }
-      for (int k = 0; k < K; ++k) {
-         const uint32_t s = __reduce_add_sync(FULL, ones.total(k));
-         if (lane == 0 && s) { atomicAdd(&sOnes[k], s); }
-      }
-   }
-   if (lane == 0 && cells) { atomicAdd(&sCells, cells); }
+// Add the CTA's counts of one field to its output rows (whole CTA; call after every warp has
+// added its cells to S.cells): mixed codes as counted, 255 from the all-ones sums, 0 = the rest.
+template <int TY, typename P>
+__device__ void ctaFlush(const P &a, ThermoShared &S, uint32_t *dyn)
+{
    __syncthreads();
-
-   const int warp = threadIdx.x >> 5;
+   const int K = a.K;
+   const uint32_t *hist = histOf<TY>(dyn);
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
    for (int k = warp; k < K; k += kThWarps) {
       uint32_t s = 0;
-      for (int c = 1 + lane; c < 255; c += 32) { s += sHist[k * 256 + c]; }
+      for (int c = 1 + lane; c < 255; c += 32) { s += hist[k * 256 + c]; }
       s = __reduce_add_sync(FULL, s);
       if (lane == 0) {
-         const unsigned long long n1 = sOnes[k];
-         const unsigned long long n0 = sCells - n1 - s;
+         const unsigned long long n1 = S.ones[k];
+         const unsigned long long n0 = S.cells - n1 - s;
          uint64_t *o = a.out + (size_t)a.outRow[k] * 256;
          const int c0 = a.complement ? 255 : 0;
          if (n0) { atomicAdd((unsigned long long *)(o + c0), n0); }
@@ -331,11 +194,231 @@ __global__ void __launch_bounds__(kThWarps * 32, TY == 8 ? THERMO_MINB : 2) ther
    }
    for (int i = threadIdx.x; i < K * 256; i += blockDim.x) {
       const int c = i & 255;
-      const uint32_t v = sHist[i];
+      const uint32_t v = hist[i];
       if (v && c != 0 && c != 255) {
          const int cc = a.complement ? 255 - c : c;
          atomicAdd((unsigned long long *)(a.out + (size_t)a.outRow[i >> 8] * 256 + cc), (unsigned long long)v);
       }
+   }
+   __syncthreads();
+}
+
+// One warp counts one work item (31 x positions, TY rows, D planes) of the field described by
+// `a` into the CTA's histogram and all-ones totals. Returns the item's number of cells.
+template <typename T, int TY, bool GE, bool SLOT2, typename P>
+__device__ __forceinline__ unsigned long long warpItem(const P &a, long long it, ThermoShared &S, uint32_t *dyn)
+{
+   constexpr int W = sizeof(T) / 4;  // 32-bit words per element; the ranked word is the last one
+   const int lane = threadIdx.x & 31;
+   uint32_t *sHist = histOf<TY>(dyn);
+   uint32_t(*stage)[TY + 1][32] = reinterpret_cast<uint32_t(*)[TY + 1][32]>(dyn + (threadIdx.x >> 5) * 2 * (TY + 1) * 32);
+   const int K = a.K;
+   const unsigned *__restrict__ F32w = reinterpret_cast<const unsigned *>(a.f) + (W - 1);
+   const long long rowStep = (long long)W * a.sy, planeStep = (long long)W * a.sz;
+   const uint32_t nanRank = a.nanRank;
+
+   const int ix = (int)(it % a.nSegX);
+   const long long rest = it / a.nSegX;
+   const int iy = (int)(rest % a.nTileY);
+   const int iz = (int)(rest / a.nTileY);
+   const int x0 = 31 * ix, y0 = TY * iy, z0 = a.D * iz;
+   const int xl = min(x0 + lane, a.X - 1);  // lanes past the row end re-read the last element
+   const uint32_t vx = ((lane < 31) && (x0 + lane < a.X - 1)) ? 0xFFFFFFFFu : 0u;
+   const int nRow = min(TY, a.Y - 1 - y0);
+   const int nPln = min(a.D, a.Z - 1 - z0);
+   const int lastRow = a.Y - 1 - y0;  // rows j > lastRow re-read row lastRow
+   const unsigned *__restrict__ P0 = F32w + (long long)W * ((long long)xl * a.sx + (long long)y0 * a.sy + (long long)z0 * a.sz);
+   const unsigned *Pn = P0;
+
+   // stage plane 0; every lane later reads back only the words it copied itself
+   {
+      const unsigned *q = Pn;
+#pragma unroll
+      for (int j = 0; j <= TY; ++j) {
+         cpAsync4(&stage[0][j][lane], q);
+         if (j < lastRow) { q += rowStep; }
+      }
+      cpAsyncCommit();
+   }
+   uint32_t sF[TY], sM[TY];  // previous plane: face ranks, min | max << 8 per row pair
+   PlaneOnes<TY> ones;
+   for (int p = 0; p <= nPln; ++p) {
+      Pn += planeStep;
+      if (p < nPln) {  // stage the next plane while this one is ranked and counted
+         const unsigned *q = Pn;
+#pragma unroll
+         for (int j = 0; j <= TY; ++j) {
+            cpAsync4(&stage[(p + 1) & 1][j][lane], q);
+            if (j < lastRow) { q += rowStep; }
+         }
+         cpAsyncCommit();
+         cpAsyncWait<1>();
+      } else {
+         cpAsyncWait<0>();
+      }
+      const uint32_t(*w)[32] = stage[p & 1];
+      uint32_t r[TY + 1];
+      uint32_t slow = 0;  // bit j: element of row j needs the exact rank
+#pragma unroll
+      for (int j = 0; j <= TY; ++j) {
+         const uint32_t wj = w[j][lane];
+         const uint32_t key = sortKey(wj);
+         const uint32_t r0 = S.lut[key >> kLutShift];
+         const uint32_t cand = S.key[r0];
+         r[j] = r0 + (GE ? (key >= cand) : (key > cand));
+         if (W == 2) {
+            slow |= (uint32_t)((key == cand) | ((key - 0x00100000u) >= 0xFFE00000u)) << j;
+         } else {
+            r[j] = ((wj & 0x7FFFFFFFu) > 0x7F800000u) ? nanRank : r[j];
+         }
+      }
+      if (W == 2 && slow) {
+         const T *Fe = reinterpret_cast<const T *>(a.f);
+         const long long e0 = (long long)xl * a.sx + (long long)y0 * a.sy + (long long)(z0 + p) * a.sz;
+#pragma unroll
+         for (int j = 0; j <= TY; ++j) {
+            if ((slow >> j) & 1u) {
+               r[j] = exactRank<T, GE>(Fe, e0 + (long long)min(j, lastRow) * a.sy, S.tlo, S.thi, K, nanRank);
+            }
+         }
+      }
+      uint32_t rR = __shfl_down_sync(FULL, r[0], 1);
+      uint32_t ePrev = __byte_perm(r[0], rR, 0x0040);
+      uint32_t mnPrev = min(r[0], rR), mxPrev = max(r[0], rR);
+      if (p == 0) {
+#pragma unroll
+         for (int j = 0; j < TY; ++j) {
+            rR = __shfl_down_sync(FULL, r[j + 1], 1);
+            const uint32_t e = __byte_perm(r[j + 1], rR, 0x0040);
+            const uint32_t mn = min(r[j + 1], rR), mx = max(r[j + 1], rR);
+            sF[j] = __byte_perm(ePrev, e, 0x5410);
+            sM[j] = min(mnPrev, mn) | (max(mxPrev, mx) << 8);
+            ePrev = e;
+            mnPrev = mn;
+            mxPrev = mx;
+         }
+         continue;
+      }
+#pragma unroll
+      for (int j = 0; j < TY; ++j) {
+         rR = __shfl_down_sync(FULL, r[j + 1], 1);
+         const uint32_t e = __byte_perm(r[j + 1], rR, 0x0040);
+         const uint32_t mn = min(r[j + 1], rR), mx = max(r[j + 1], rR);
+         const uint32_t fc = __byte_perm(ePrev, e, 0x5410);
+         const uint32_t fmn = min(mnPrev, mn), fmx = max(mxPrev, mx);
+         const uint32_t rmin = min(sM[j] & 0xFFu, fmn);
+         const uint32_t vmask = (j < nRow) ? vx : 0u;
+         const uint32_t rmax = vmask ? max(sM[j] >> 8, fmx) : rmin;  // invalid cells: no mixed codes
+         ones.add(j, thermo(rmin) & vmask);
+         {
+            // codes of the cell for k = rmin and rmin + 1, predicated (no branch); the rare
+            // cells spanning more thresholds finish in a loop
+            const uint32_t R0 = sF[j], R1 = fc;
+            const uint32_t C0 = 0x7F7F7F7Fu - rmin * 0x01010101u;
+            uint32_t *h = sHist + (rmin << 8);
+            {
+               const uint32_t t0 = (R0 + C0) & 0x80808080u;
+               const uint32_t t1 = (R1 + C0) & 0x80808080u;
+               const uint32_t c = ((t0 * 0x00204081u) >> 28) | (((t1 * 0x00204081u) >> 24) & 0xF0u);
+               if (rmin < rmax) { atomicAdd(h + c, 1u); }
+            }
+            if (SLOT2) {
+               const uint32_t C1 = C0 - 0x01010101u;
+               const uint32_t t0 = (R0 + C1) & 0x80808080u;
+               const uint32_t t1 = (R1 + C1) & 0x80808080u;
+               const uint32_t c = ((t0 * 0x00204081u) >> 28) | (((t1 * 0x00204081u) >> 24) & 0xF0u);
+               if (rmin + 1 < rmax) { atomicAdd(h + 256 + c, 1u); }
+               if (rmin + 2 < rmax) {
+                  uint32_t C = C1 - 0x01010101u;
+                  uint32_t *hk = h + 512;
+                  uint32_t k = rmin + 2;
+                  do {
+                     const uint32_t u0 = (R0 + C) & 0x80808080u;
+                     const uint32_t u1 = (R1 + C) & 0x80808080u;
+                     const uint32_t cc = ((u0 * 0x00204081u) >> 28) | (((u1 * 0x00204081u) >> 24) & 0xF0u);
+                     atomicAdd(hk + cc, 1u);
+                     C -= 0x01010101u;
+                     hk += 256;
+                  } while (++k < rmax);
+               }
+            }
+         }
+         sF[j] = fc;
+         sM[j] = fmn | (fmx << 8);
+         ePrev = e;
+         mnPrev = mn;
+         mxPrev = mx;
+      }
+   }
+   for (int k = 0; k < K; ++k) {
+      const uint32_t s = __reduce_add_sync(FULL, ones.total(k));
+      if (lane == 0 && s) { atomicAdd(&S.ones[k], s); }
+   }
+   return (unsigned long long)max(0, min(31, a.X - 1 - x0)) * (unsigned)nRow * (unsigned)nPln;
+}
+
+template <typename T, int TY, bool GE, bool SLOT2>
+__global__ void __launch_bounds__(kThWarps * 32, TY == 8 ? THERMO_MINB : 2) thermoBPFD(const __grid_constant__ FusedArgs a)
+{
+   __shared__ ThermoShared S;
+   extern __shared__ uint32_t sDyn[];
+   ctaSetup<TY>(a, S, sDyn);
+   const long long gw = (long long)blockIdx.x * kThWarps + (threadIdx.x >> 5);
+   const long long nw = (long long)gridDim.x * kThWarps;
+   unsigned long long cells = 0;
+   for (long long it = gw; it < a.nItems; it += nw) { cells += warpItem<T, TY, GE, SLOT2>(a, it, S, sDyn); }
+   if ((threadIdx.x & 31) == 0 && cells) { atomicAdd(&S.cells, cells); }
+   ctaFlush<TY>(a, S, sDyn);
+}
+
+// ---------------------------------------------------------------- many fields, one launch
+
+// A CTA takes chunks of consecutive work items from a global counter; chunks never span fields.
+// When the next chunk belongs to another field, the CTA adds its counts of the previous field to
+// that field's output rows, then loads the new field's thresholds and rank table.
+template <int TY>
+__global__ void __launch_bounds__(kThWarps * 32, THERMO_MINB) thermoBatch(const __grid_constant__ BatchArgs b)
+{
+   __shared__ ThermoShared S;
+   __shared__ FieldTask F;
+   __shared__ int sChunk;
+   extern __shared__ uint32_t sDyn[];
+   int cur = -1;
+   unsigned long long cells = 0;
+   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+   for (;;) {
+      if (threadIdx.x == 0) { sChunk = (int)atomicAdd(b.counter, 1u); }
+      __syncthreads();
+      const int c = sChunk;
+      __syncthreads();
+      if (c >= b.nChunks) { break; }
+      const BatchChunk ch = b.chunks[c];
+      if (ch.field != cur) {
+         if (cur >= 0) {
+            if (lane == 0 && cells) { atomicAdd(&S.cells, cells); }
+            cells = 0;
+            ctaFlush<TY>(F, S, sDyn);
+         }
+         const uint32_t *src = reinterpret_cast<const uint32_t *>(b.tasks + ch.field);
+         for (int i = threadIdx.x; i < (int)(sizeof(FieldTask) / 4); i += blockDim.x) {
+            reinterpret_cast<uint32_t *>(&F)[i] = src[i];
+         }
+         __syncthreads();
+         ctaSetup<TY>(F, S, sDyn);
+         cur = ch.field;
+      }
+      for (long long it = ch.begin + warp; it < ch.end; it += kThWarps) {
+         switch (F.variant) {
+            case 0: cells += warpItem<float, TY, false, true>(F, it, S, sDyn); break;
+            case 1: cells += warpItem<float, TY, true, true>(F, it, S, sDyn); break;
+            case 2: cells += warpItem<double, TY, false, true>(F, it, S, sDyn); break;
+            default: cells += warpItem<double, TY, true, true>(F, it, S, sDyn); break;
+         }
+      }
+   }
+   if (cur >= 0) {
+      if (lane == 0 && cells) { atomicAdd(&S.cells, cells); }
+      ctaFlush<TY>(F, S, sDyn);
    }
 }
 
@@ -379,22 +462,66 @@ static int launchThermoT(const FusedArgs &a, cudaStream_t s)
    return cudaFail(cudaGetLastError(), "thermoBPFD launch");
 }
 
-int launchThermo(FusedArgs &a, int enc, cudaStream_t s)
+// Fill the key table of a thermometer pass; returns false when two thresholds share a bucket of
+// the rank table (such passes use the binary-search kernel of fused.cu).
+template <typename P>
+static bool prepareKeys(P &a, int enc)
 {
    const bool ge = a.rankHi != 0;
    for (int k = 0; k < a.K; k++) { a.tkey[k] = thresholdKey(ge ? a.thi[k] : a.tlo[k], enc, ge); }
-   // the table needs at most one threshold key per bucket
-   a.lutOk = 1;
    for (int k = 0; k + 1 < a.K; k++) {
-      if ((a.tkey[k] >> kLutShift) == (a.tkey[k + 1] >> kLutShift)) { a.lutOk = 0; }
+      if ((a.tkey[k] >> kLutShift) == (a.tkey[k + 1] >> kLutShift)) { return false; }
    }
-   if (!a.lutOk) { return MKF_ERR_UNSUPPORTED; }
+   return true;
+}
+
+// Work-item grid of a field for the thermometer kernels (TY rows, D planes, 31 cells per item).
+template <typename P>
+static void itemGrid(P &a, int D)
+{
    constexpr int TY = THERMO_TY;
-   a.D = 32;
+   a.D = D;
    a.nSegX = (a.X - 1 + 30) / 31;
    a.nTileY = (a.Y - 1 + TY - 1) / TY;
    a.nSlabZ = (a.Z - 1 + a.D - 1) / a.D;
    a.nItems = (long long)a.nSegX * a.nTileY * a.nSlabZ;
+}
+
+bool prepareThermoTask(FieldTask &t, int enc)
+{
+   t.variant = (enc == ENC_F32 ? 0 : 2) + (t.rankHi ? 1 : 0);
+   if (!prepareKeys(t, enc)) { return false; }
+   itemGrid(t, 32);
+   return true;
+}
+
+int launchThermoBatch(const BatchArgs &b, cudaStream_t s)
+{
+   constexpr int TY = THERMO_TY;
+   static int blocksPerSM = -1;
+   auto kern = thermoBatch<TY>;
+   const size_t stageBytes = (size_t)kThWarps * 2 * (TY + 1) * 32 * sizeof(uint32_t);
+   const size_t smem = stageBytes + (size_t)MKF_MAX_THRESH * 256 * 4;
+   if (blocksPerSM < 0) {
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      int n = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, kThWarps * 32, smem);
+      blocksPerSM = n > 0 ? n : 1;
+   }
+   long long grid = (long long)smCount() * blocksPerSM;
+   if (grid > b.nChunks) { grid = b.nChunks; }
+   if (grid < 1) { grid = 1; }
+   kern<<<(unsigned)grid, kThWarps * 32, smem, s>>>(b);
+   return cudaFail(cudaGetLastError(), "thermoBatch launch");
+}
+
+int launchThermo(FusedArgs &a, int enc, cudaStream_t s)
+{
+   a.lutOk = prepareKeys(a, enc) ? 1 : 0;
+   if (!a.lutOk) { return MKF_ERR_UNSUPPORTED; }
+   constexpr int TY = THERMO_TY;
+   itemGrid(a, 32);
+   const bool ge = a.rankHi != 0;
    // one threshold: a cell has at most one mixed code
    if (a.K == 1) {
       if (enc == ENC_F32) { return ge ? launchThermoT<float, TY, true, false>(a, s) : launchThermoT<float, TY, false, false>(a, s); }

@@ -300,6 +300,53 @@ def test_batch_equals_per_field(mkf, cuda):
         row += len(t)
 
 
+def test_batch_plan_mixed_fields_and_graph(mkf, oracle, cuda):
+    """A batch with FP32/FP64 fields, every relation, constant maps, NaN thresholds and a strided
+    view; plan launches, graph replays, and a replay after the fields' contents change."""
+    import torch
+
+    rng = np.random.default_rng(37)
+    fields, ts, ms = [], [], []
+    for i in range(14):
+        shape = (int(rng.integers(2, 40)), int(rng.integers(2, 40)), int(rng.choice([17, 31, 32, 33, 64, 90])))
+        dtype = (np.float32, np.float64)[i % 2]
+        fields.append(to_dev((rng.standard_normal(shape) * 1.5).astype(dtype), cuda))
+        K = int(rng.integers(1, 9))
+        t = rng.standard_normal(K)
+        if i % 4 == 3:
+            m = rng.integers(0, 8, size=K).astype(np.uint32)  # mixed relations: the field's own pass
+            t[0] = np.nan
+        else:
+            m = int(rng.choice([1, 3, 4, 6]))
+        ts.append(t)
+        ms.append(m)
+    big = to_dev(rng.standard_normal((20, 30, 50)), cuda)
+    fields.append(big[2:18, 3:27, 5:45])  # strided view
+    ts.append(np.array([0.2, -0.4]))
+    ms.append(4)
+
+    def want():
+        return [oracle.bpfd_field(np.ascontiguousarray(f.cpu().numpy()), tuple(f.shape[::-1]), t,
+                                  m if np.ndim(m) else [m] * len(t))
+                for f, t, m in zip(fields, ts, ms)]
+
+    plan = mkf.BatchPlan(fields, ts, ms)
+    for launch in (plan.launch, plan.launch, plan.launch_graph, plan.launch_graph):
+        got = u64(launch())
+        row = 0
+        for w in want():
+            assert (got[row:row + len(w)] == w).all()
+            row += len(w)
+    for f in fields:
+        f.mul_(-1.0)  # new contents, same buffers
+    got = u64(plan.launch_graph())
+    row = 0
+    for w in want():
+        assert (got[row:row + len(w)] == w).all()
+        row += len(w)
+    plan.close()
+
+
 def test_device_measures_equal_host(mkf, golden, cuda):
     import torch
 
