@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--impl", default="mkf", choices=["mkf", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true", help="skip the batched and serving workloads")
     return ap.parse_args()
 
 
@@ -96,6 +97,102 @@ def grf_numpy(nz, ny, nx, seed):
     f -= f.mean()
     f /= f.std()
     return np.ascontiguousarray(f.ravel())
+
+
+def ball_fields(n_fields, seed, device, lo=17, hi=400, dtype=None):
+    """The uneven batch: each axis uniform in [lo, hi]; content = max over 1-64 balls (centres
+    uniform in the box, radii uniform in [2, 40]) of r - |x - c|, plus N(0, 0.1) noise. The max
+    is formed inside each ball's bounding box only: elsewhere the value stays far below zero,
+    which maps the same at threshold 0."""
+    import torch
+
+    dtype = dtype or torch.float32
+    rng = np.random.default_rng(seed)
+    g = torch.Generator(device=device).manual_seed(seed)
+    fields = []
+    for _ in range(n_fields):
+        X, Y, Z = (int(v) for v in rng.integers(lo, hi + 1, size=3))
+        f = torch.full((Z, Y, X), -50.0, dtype=dtype, device=device)
+        for _b in range(int(rng.integers(1, 65))):
+            c = rng.random(3) * np.array([X, Y, Z])
+            r = float(rng.uniform(2, 40))
+            lo3 = [max(0, int(np.floor(c[i] - r - 1))) for i in range(3)]
+            hi3 = [min((X, Y, Z)[i], int(np.ceil(c[i] + r + 2))) for i in range(3)]
+            if min(hi3[i] - lo3[i] for i in range(3)) <= 0:
+                continue
+            zz = torch.arange(lo3[2], hi3[2], device=device, dtype=dtype).view(-1, 1, 1) - c[2]
+            yy = torch.arange(lo3[1], hi3[1], device=device, dtype=dtype).view(1, -1, 1) - c[1]
+            xx = torch.arange(lo3[0], hi3[0], device=device, dtype=dtype).view(1, 1, -1) - c[0]
+            v = r - torch.sqrt(zz * zz + yy * yy + xx * xx)
+            box = f[lo3[2]:hi3[2], lo3[1]:hi3[1], lo3[0]:hi3[0]]
+            torch.maximum(box, v, out=box)
+        f.add_(torch.randn((Z, Y, X), dtype=dtype, device=device, generator=g).mul_(0.1))
+        fields.append(f)
+    torch.cuda.synchronize(device)
+    return fields
+
+
+def run_batch_workload(dev, n_fields=512, seed=SEED + 3, reps=3):
+    """Uneven batch (512 FP32 fields, threshold 0): fields/s of the plain drop-in call per field
+    (binMapCUDA + mkfCUDAGetBPFDH), of the fused call per field (mkfFieldBPFD), and of one
+    batched launch (mkfBatchPlanLaunch, and replayed as a CUDA graph)."""
+    import torch
+
+    import mkf_b200
+
+    fields = ball_fields(n_fields, seed, dev)
+    vox = sum(f.numel() for f in fields)
+    t = [0.0]
+    # plain drop-in: one map + one count + one host copy per field, synchronous
+    mkf_b200.get_bpfd_host(*mkf_b200.bin_map_cuda(fields[0], ">", 0.0)[:2])
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for f in fields:
+        pbm, org, _ = mkf_b200.bin_map_cuda(f, ">", 0.0)
+        mkf_b200.get_bpfd_host(pbm, org)
+    plain_s = time.perf_counter() - t0
+    # fused per field (asynchronous calls, one synchronisation at the end)
+    outs = [torch.zeros((1, 256), dtype=torch.int64, device=dev) for _ in fields]
+    for f, o in zip(fields, outs):
+        mkf_b200.field_bpfd(f, t, mkf_b200.BMC_GT, out=o)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for f, o in zip(fields, outs):
+        mkf_b200.field_bpfd(f, t, mkf_b200.BMC_GT, out=o)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    fused_s = e0.elapsed_time(e1) * 1e-3
+    # batched: one launch (and a CUDA graph replay) for all fields
+    plan = mkf_b200.BatchPlan(fields, [t] * len(fields))
+    plan.launch()
+    plan.launch_graph()
+    torch.cuda.synchronize(dev)
+    times = {}
+    for name, fn in (("batched", plan.launch), ("batched_graph", plan.launch_graph)):
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        times[name] = e0.elapsed_time(e1) * 1e-3 / reps
+    # the batched counts equal the per-field ones
+    same = bool(torch.equal(plan.out, torch.cat(outs)))
+    plan.close()
+    res = {
+        "workload": f"{n_fields} FP32 fields, axes U[17,400], balls + N(0,0.1) noise, threshold 0 (>)",
+        "voxels": int(vox),
+        "plain_dropin_fields_per_s": n_fields / plain_s,
+        "fused_per_field_fields_per_s": n_fields / fused_s,
+        "batched_fields_per_s": n_fields / times["batched"],
+        "batched_graph_fields_per_s": n_fields / times["batched_graph"],
+        "batched_gvoxel_per_s": vox / times["batched"] * 1e-9,
+        "batched_vs_plain": plain_s / times["batched"],
+        "batched_equals_per_field": same,
+    }
+    del fields, outs
+    torch.cuda.empty_cache()
+    return res
 
 
 # ---------------------------------------------------------------- clocks
@@ -380,6 +477,9 @@ def run_mkf(args, rank, world, local_rank):
     }
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(fh_np.reshape(-1))
+    if world == 1 and not args.no_secondary:
+        del fh, fh_np
+        line["batched"] = run_batch_workload(dev)
     print(json.dumps(line), flush=True)
 
 

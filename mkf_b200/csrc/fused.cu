@@ -477,6 +477,13 @@ int fieldBPFD(uint64_t *out, const MKFFieldDesc *pF, const MKFThreshSet *pT, int
          a.nanRank = (eqBit != (ps.complement != 0)) ? (uint32_t)a.K : 0u;
       }
       a.out = out;
+      if (a.K <= 2) {
+         uint32_t masks[MKF_MAX_THRESH];
+         for (int k = 0; k < a.K; k++) { masks[k] = ps.mask[idx[k]]; }
+         rc = launchWords(a, pF->enc, masks, s);
+         if (rc != MKF_OK) { return rc; }
+         continue;
+      }
       constexpr int TY = 16;
       a.D = 64;
       a.nSegX = (X - 1 + 30) / 31;

@@ -67,6 +67,10 @@ bool planBatchField(const MKFFieldDesc *pF, const MKFThreshSet *pT, int rowBase,
 bool prepareThermoTask(FieldTask &t, int enc);
 int launchThermoBatch(const BatchArgs &b, cudaStream_t s);
 
+// Word-parallel kernel for one or two thresholds of any relations (words.cu); `masks` are the
+// relation masks of f's (sorted) thresholds. MKF_ERR_UNSUPPORTED for other K.
+int launchWords(const FusedArgs &f, int enc, const uint32_t *masks, cudaStream_t s);
+
 // Launch the thermometer kernel for a pass whose thresholds all share one relation
 // (< <= > >=); fills the key table of `a` first.
 int launchThermo(FusedArgs &a, int enc, cudaStream_t s);

@@ -1,0 +1,288 @@
+// words.cu - fused counting kernel for one or two thresholds (any relations), word-parallel.
+//
+// With few thresholds the per-element cost must be a handful of instructions, so cells are
+// handled 32 at a time as bit words, as the original's packed binary map does
+// (bpfdCUDA.cuh:41-118), but without storing the map. A warp item is a tile of 32 x positions
+// (31 cells), 32 rows (31 row pairs) and D planes, walked plane by plane:
+//  * load: lane = x; the warp issues the 32 rows' coalesced loads at once;
+//  * pack: one ballot per row and threshold gives that row's 32-bit map word; lane r keeps row r's;
+//  * count: lane = row pair. A cell's eight corners are bits b and b+1 of four words (this lane's
+//    row and the next lane's row, previous and current plane), so all-ones and all-zeros cells
+//    are popcounts of ANDs and ORs of the words and their one-bit shifts; only mixed cells form
+//    their 8-bit code, counted in a per-CTA shared histogram.
+#include <cmath>
+#include <cstring>
+#include <type_traits>
+#include "fused.cuh"
+
+namespace mkf {
+
+#ifndef WORDS_MINB_F32
+#define WORDS_MINB_F32 4
+#endif
+
+static constexpr int kWdWarps = 8;
+static constexpr int kWdD = 32;
+
+// Relation class of a threshold: every class is one comparison (NaN maps as the EQ bit says).
+enum WordCls { kGT = 0, kGE = 1, kLT = 2, kLE = 3, kGEN = 4 };
+
+struct WordArgs
+{
+   const void *f;
+   int64_t sx, sy, sz;
+   int X, Y, Z;
+   int K;                 // 1 or 2
+   int cls[2];
+   uint32_t m[2];         // relation masks (GEN)
+   double tlo[2], thi[2]; // exact-equivalent thresholds for "f > t" / "f >= t" tests
+   int outRow[2];
+   uint64_t *out;
+   int nChunkX, nTileY, nSlabZ;
+   long long nItems;
+};
+
+template <typename T>
+__device__ __forceinline__ uint32_t mapBit(T v, int cls, uint32_t m, T tlo, T thi)
+{
+   switch (cls) {
+      case kGT: return v > tlo;
+      case kGE: return !(v < thi);
+      case kLT: return v < thi;
+      case kLE: return !(v > tlo);
+      default: {
+         const uint32_t d = 1u - (uint32_t)(v < thi) + (uint32_t)(v > tlo);
+         return (m >> d) & 1u;
+      }
+   }
+}
+
+// State of one warp item between planes: the previous plane's map words and the cell counts.
+template <int KMAX>
+struct WordCarry
+{
+   uint32_t pw[KMAX], pn[KMAX];  // previous plane: this lane's row word and the next row's
+   uint32_t n0[KMAX], n1[KMAX];  // all-zeros and all-ones cells counted by this lane
+};
+
+// Load one plane's 32 x 32 tile (lane = x). INNER: every row of the tile lies inside the field
+// and the row stride in bytes `syb` times 31 fits 32 bits, so each row address is one multiply-add
+// on the plane pointer; otherwise rows past the field end repeat its last row (their cells are
+// masked out when counted) and addresses are formed in 64 bits.
+template <typename T, bool INNER>
+__device__ __forceinline__ void loadPlane(T (&v)[32], const T *__restrict__ p, int64_t sy, uint32_t syb, int nRow)
+{
+#pragma unroll
+   for (int r = 0; r < 32; r++) {
+      if (INNER) {
+         v[r] = __ldg((const T *)((const char *)p + (uint64_t)(syb * (uint32_t)r)));
+      } else {
+         v[r] = __ldg(p + (int64_t)min(r, nRow - 1) * sy);
+      }
+   }
+}
+
+// Map, pack and count one plane (see the file comment). `first`: no previous plane yet.
+// `sRow` is the warp's 32-word transposition buffer per threshold.
+template <typename T, int KMAX, int CLS0, int CLS1>
+__device__ __forceinline__ void countPlane(const T (&v)[32], WordCarry<KMAX> &c, const WordArgs &a, const T *tlo,
+                                           const T *thi, bool xin, int lane, uint32_t vm, bool first,
+                                           uint32_t (*sRow)[32], uint32_t *sHist)
+{
+#pragma unroll
+   for (int r = 0; r < 32; r++) {
+#pragma unroll
+      for (int k = 0; k < KMAX; k++) {
+         const int cls = k == 0 ? CLS0 : CLS1;
+         // every lane stores the same (warp-uniform) word
+         sRow[k][r] = __ballot_sync(FULL, xin && mapBit<T>(v[r], cls, a.m[k], tlo[k], thi[k]));
+      }
+   }
+   __syncwarp();
+   uint32_t cw[KMAX];
+#pragma unroll
+   for (int k = 0; k < KMAX; k++) { cw[k] = sRow[k][lane]; }
+   __syncwarp();
+#pragma unroll
+   for (int k = 0; k < KMAX; k++) {
+      const uint32_t cn = __shfl_down_sync(FULL, cw[k], 1);
+      if (!first) {
+         const uint32_t a0 = c.pw[k], a1 = c.pn[k], a2 = cw[k], a3 = cn;
+         const uint32_t all = a0 & (a0 >> 1) & a1 & (a1 >> 1) & a2 & (a2 >> 1) & a3 & (a3 >> 1) & vm;
+         const uint32_t any = a0 | (a0 >> 1) | a1 | (a1 >> 1) | a2 | (a2 >> 1) | a3 | (a3 >> 1);
+         c.n1[k] += __popc(all);
+         c.n0[k] += __popc(vm & ~any);
+         uint32_t mixed = vm & any & ~all;
+         if (mixed) {
+            // word j's bits b, b+1 go to code bits 2j, 2j+1: pre-shift j's word left by 2j as a
+            // 64-bit (hi:lo) pair, so one funnel shift by b brings them into place
+            const uint32_t l1 = a1 << 2, h1 = a1 >> 30, l2 = a2 << 4, h2 = a2 >> 28, l3 = a3 << 6, h3 = a3 >> 26;
+            uint32_t *hk = sHist + k * 256;
+            do {
+               const int b = 31 - __clz(mixed);
+               mixed ^= 1u << b;
+               uint32_t code = (__funnelshift_r(l1, h1, b) & ~3u) | ((a0 >> b) & 3u);
+               code = (__funnelshift_r(l2, h2, b) & ~15u) | (code & 15u);
+               code = (__funnelshift_r(l3, h3, b) & ~63u) | (code & 63u);
+               atomicAdd(hk + (code & 255u), 1u);
+            } while (mixed);
+         }
+      }
+      c.pw[k] = cw[k];
+      c.pn[k] = cn;
+   }
+}
+
+// One launch counts K = KMAX thresholds of classes CLS0 (and CLS1), compile-time constants.
+// INNER: the field is at least 32 x 32 in x and y with a positive row stride below 2^32 / 31
+// bytes; edge tiles are then shifted back inside the field (their cells already counted by the
+// neighbouring tile are masked out), so no load needs clamping.
+template <typename T, int KMAX, int CLS0, int CLS1, bool INNER, int MINB>
+__global__ void __launch_bounds__(kWdWarps * 32, MINB) wordBPFD(const __grid_constant__ WordArgs a)
+{
+   __shared__ uint32_t sHist[KMAX * 256];
+   __shared__ unsigned long long sEnds[KMAX][2];  // all-zeros, all-ones cells
+   __shared__ uint32_t sRows[kWdWarps][KMAX][32];
+   for (int i = threadIdx.x; i < KMAX * 256; i += blockDim.x) { sHist[i] = 0; }
+   if (threadIdx.x < KMAX * 2) { (&sEnds[0][0])[threadIdx.x] = 0; }
+   __syncthreads();
+
+   T tlo[KMAX], thi[KMAX];
+#pragma unroll
+   for (int k = 0; k < KMAX; k++) {
+      tlo[k] = (T)a.tlo[k];
+      thi[k] = (T)a.thi[k];
+   }
+   const int lane = threadIdx.x & 31;
+   const long long gw = (long long)blockIdx.x * kWdWarps + (threadIdx.x >> 5);
+   const long long nw = (long long)gridDim.x * kWdWarps;
+   const T *__restrict__ F = (const T *)a.f;
+   const uint32_t syb = (uint32_t)(a.sy * (int64_t)sizeof(T));
+   uint32_t (*sRow)[32] = sRows[threadIdx.x >> 5];
+
+   for (long long it = gw; it < a.nItems; it += nw) {
+      const int ix = (int)(it % a.nChunkX);
+      const long long rest = it / a.nChunkX;
+      const int iy = (int)(rest % a.nTileY);
+      const int iz = (int)(rest / a.nTileY);
+      // this item's cells: x in [xs, xe), y in [ys, ye), z in [z0, z0 + nPln)
+      const int xs = 31 * ix, ys = 31 * iy, z0 = kWdD * iz;
+      const int xe = min(xs + 31, a.X - 1), ye = min(ys + 31, a.Y - 1);
+      const int nPln = min(kWdD, a.Z - 1 - z0);
+      // tile origin: bit b of a word is x0 + b, lane l counts the row pair y0 + l
+      const int x0 = INNER ? min(xs, a.X - 32) : xs;
+      const int y0 = INNER ? min(ys, a.Y - 32) : ys;
+      const int nRow = INNER ? 32 : min(32, a.Y - y0);
+      const bool xin = INNER || x0 + lane < a.X;
+      const T *base = F + (long long)(INNER ? x0 + lane : min(x0 + lane, a.X - 1)) * a.sx + (long long)y0 * a.sy +
+                      (long long)z0 * a.sz;
+      const uint32_t vm = (y0 + lane >= ys && y0 + lane < ye)
+                             ? ((0xFFFFFFFFu >> (32 - (xe - x0))) & (0xFFFFFFFFu << (xs - x0)))
+                             : 0u;
+      WordCarry<KMAX> c;
+#pragma unroll
+      for (int k = 0; k < KMAX; k++) { c.n0[k] = c.n1[k] = 0; c.pw[k] = c.pn[k] = 0; }
+      for (int p = 0; p <= nPln; ++p) {
+         T v[32];
+         loadPlane<T, INNER>(v, base + (long long)p * a.sz, a.sy, syb, nRow);
+         countPlane<T, KMAX, CLS0, CLS1>(v, c, a, tlo, thi, xin, lane, vm, p == 0, sRow, sHist);
+      }
+#pragma unroll
+      for (int k = 0; k < KMAX; k++) {
+         const unsigned long long s0 = __reduce_add_sync(FULL, c.n0[k]);
+         const unsigned long long s1 = __reduce_add_sync(FULL, c.n1[k]);
+         if (lane == 0) {
+            if (s0) { atomicAdd(&sEnds[k][0], s0); }
+            if (s1) { atomicAdd(&sEnds[k][1], s1); }
+         }
+      }
+   }
+   __syncthreads();
+   for (int i = threadIdx.x; i < KMAX * 256; i += blockDim.x) {
+      const int k = i >> 8, c = i & 255;
+      unsigned long long v = sHist[i];
+      if (c == 0) { v += sEnds[k][0]; }
+      if (c == 255) { v += sEnds[k][1]; }
+      if (v) { atomicAdd((unsigned long long *)(a.out + (size_t)a.outRow[k] * 256 + c), v); }
+   }
+}
+
+template <typename T, int KMAX, int CLS0, int CLS1, bool INNER>
+static int launchWordsI(const WordArgs &a, cudaStream_t s)
+{
+   static int blocksPerSM = -1;
+   auto kern = wordBPFD<T, KMAX, CLS0, CLS1, INNER, (INNER && sizeof(T) == 4) ? WORDS_MINB_F32 : 2>;
+   if (blocksPerSM < 0) {
+      int n = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, kWdWarps * 32, 0);
+      blocksPerSM = n > 0 ? n : 1;
+   }
+   long long grid = (a.nItems + kWdWarps - 1) / kWdWarps;
+   const long long cap = (long long)smCount() * blocksPerSM;
+   if (grid > cap) { grid = cap; }
+   if (grid < 1) { grid = 1; }
+   kern<<<(unsigned)grid, kWdWarps * 32, 0, s>>>(a);
+   return cudaFail(cudaGetLastError(), "wordBPFD launch");
+}
+
+template <typename T, int KMAX, int CLS0, int CLS1>
+static int launchWordsT(const WordArgs &a, cudaStream_t s)
+{
+   const int64_t syb = a.sy * (int64_t)sizeof(T);
+   const bool inner = a.X >= 32 && a.Y >= 32 && syb > 0 && syb * 31 < (int64_t)1 << 32;
+   return inner ? launchWordsI<T, KMAX, CLS0, CLS1, true>(a, s) : launchWordsI<T, KMAX, CLS0, CLS1, false>(a, s);
+}
+
+template <typename T>
+static int dispatchWords(const WordArgs &a, cudaStream_t s)
+{
+   if (a.K == 2) {
+      if (a.cls[0] == a.cls[1]) {
+         switch (a.cls[0]) {
+            case kGT: return launchWordsT<T, 2, kGT, kGT>(a, s);
+            case kGE: return launchWordsT<T, 2, kGE, kGE>(a, s);
+            case kLT: return launchWordsT<T, 2, kLT, kLT>(a, s);
+            case kLE: return launchWordsT<T, 2, kLE, kLE>(a, s);
+            default: break;
+         }
+      }
+      return launchWordsT<T, 2, kGEN, kGEN>(a, s);
+   }
+   switch (a.cls[0]) {
+      case kGT: return launchWordsT<T, 1, kGT, kGT>(a, s);
+      case kGE: return launchWordsT<T, 1, kGE, kGE>(a, s);
+      case kLT: return launchWordsT<T, 1, kLT, kLT>(a, s);
+      case kLE: return launchWordsT<T, 1, kLE, kLE>(a, s);
+      default: return launchWordsT<T, 1, kGEN, kGEN>(a, s);
+   }
+}
+
+// Count a field for K = 1 or 2 thresholds (sorted or not; tlo/thi/masks per threshold, rows in
+// outRow). Returns MKF_ERR_UNSUPPORTED for other K.
+int launchWords(const FusedArgs &f, int enc, const uint32_t *masks, cudaStream_t s)
+{
+   if (f.K < 1 || f.K > 2) { return MKF_ERR_UNSUPPORTED; }
+   WordArgs a;
+   memset(&a, 0, sizeof(a));
+   a.f = f.f;
+   a.sx = f.sx; a.sy = f.sy; a.sz = f.sz;
+   a.X = f.X; a.Y = f.Y; a.Z = f.Z;
+   a.K = f.K;
+   a.out = f.out;
+   for (int k = 0; k < f.K; k++) {
+      const uint32_t m = masks[k] & BMC_AL;
+      a.m[k] = m;
+      a.cls[k] = (m == BMC_GT) ? kGT : (m == (BMC_GT | BMC_EQ)) ? kGE : (m == BMC_LT) ? kLT : (m == (BMC_LT | BMC_EQ)) ? kLE : kGEN;
+      a.tlo[k] = f.tlo[k];
+      a.thi[k] = f.thi[k];
+      a.outRow[k] = f.outRow[k];
+   }
+   a.nChunkX = (a.X - 1 + 30) / 31;
+   a.nTileY = (a.Y - 1 + 30) / 31;
+   a.nSlabZ = (a.Z - 1 + kWdD - 1) / kWdD;
+   a.nItems = (long long)a.nChunkX * a.nTileY * a.nSlabZ;
+   if (enc == ENC_F32) { return dispatchWords<float>(a, s); }
+   return dispatchWords<double>(a, s);
+}
+
+}  // namespace mkf

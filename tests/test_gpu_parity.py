@@ -126,6 +126,34 @@ def test_fused_strided_view(mkf, oracle, cuda):
     assert (got == oracle.bpfd_field(subt, (X, Y, Z), [0.1], 6)).all()
 
 
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_fused_one_or_two_thresholds_every_relation(mkf, oracle, cuda, dtype):
+    """The word-parallel path: K = 1, 2 with every relation pair, ties, NaN. Fields narrower than
+    32 in x or y take the clamped tiles; larger ones the shifted edge tiles (x and y not multiples
+    of 31), strided views both."""
+    rng = np.random.default_rng(71)
+    for shape in [(9, 11, 64), (7, 13, 100), (5, 6, 1030), (6, 9, 33), (4, 5, 2), (3, 40, 993),
+                  (5, 45, 100), (4, 64, 64), (3, 33, 32), (34, 32, 63)]:
+        f = (rng.integers(-4, 5, size=shape) * 0.5).astype(dtype)
+        f.ravel()[rng.choice(f.size, max(1, f.size // 50), replace=False)] = np.nan
+        Z, Y, X = shape
+        for m0 in range(8):
+            m1 = (m0 * 5 + 3) % 8
+            for t in ([0.5], [0.0, -1.0]):
+                m = [m0, m1][: len(t)]
+                got = u64(mkf.field_bpfd(to_dev(f, cuda), t, m))
+                assert (got == oracle.bpfd_field(f, (X, Y, Z), t, m)).all(), (shape, m, t)
+    big = to_dev(rng.standard_normal((12, 30, 140)).astype(dtype), cuda)
+    big2 = to_dev(rng.standard_normal((10, 70, 150)).astype(dtype), cuda)
+    for view in (big[1:11, 2:28, 4:132], big[:, :, ::2], big.permute(0, 2, 1),
+                 big2[1:9, 3:67, 5:140], big2[:, :, ::2], big2.permute(0, 2, 1), big2.permute(2, 1, 0)):
+        sub = np.ascontiguousarray(view.cpu().numpy())
+        Z, Y, X = sub.shape
+        for t, m in (([0.1], [4]), ([0.1, -0.2], [6, 1])):
+            got = u64(mkf.field_bpfd(view, t, m))
+            assert (got == oracle.bpfd_field(sub, (X, Y, Z), t, m)).all()
+
+
 def test_fused_accumulate(mkf, cuda):
     rng = np.random.default_rng(3)
     f = to_dev(rng.standard_normal((20, 30, 40)), cuda)
@@ -161,6 +189,10 @@ def test_full_size_multi_threshold_properties(mkf, oracle, cuda):
     blk = f[100:164, 300:364, 700:764].contiguous()
     hb = u64(mkf.field_bpfd(blk, t, 4))
     assert (hb == oracle.bpfd_field(blk.cpu().numpy(), (64, 64, 64), t, 4)).all()
+    # one and two thresholds (the word-parallel kernel) agree with rows of the 16-threshold pass
+    assert (u64(mkf.field_bpfd(f, t[7:8], 4)) == h_gt[7:8]).all()
+    assert (u64(mkf.field_bpfd(f, t[3:5], 4)) == h_gt[3:5]).all()
+    assert (u64(mkf.field_bpfd(f, t[3:5], 3)) == h_le[3:5]).all()
     del f
 
 
