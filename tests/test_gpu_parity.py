@@ -386,3 +386,23 @@ def test_device_measures_equal_host(mkf, golden, cuda):
     dev = mkf.measures_dev(torch.from_numpy(hs.view(np.int64)).to(cuda)).cpu().numpy()
     host = mkf.measures(hs)
     assert (dev == host).all()
+
+
+# ---------------------------------------------------------------- z-slab shards (multi-GPU form, one GPU)
+
+def test_slab_shards_sum_to_whole_field(mkf, oracle, cuda):
+    """The per-rank work of the sharded form: slabs cut by slab_planes, counted one after another
+    on one GPU with no process group, sum to the whole field's counts."""
+    from mkf_b200.shard import sharded_field_bpfd, slab_planes
+
+    rng = np.random.default_rng(12)
+    f = rng.standard_normal((50, 70, 90))
+    fd = to_dev(f, cuda)
+    t = [-0.5, 0.0, 0.7]
+    want = oracle.bpfd_field(f, (90, 70, 50), t, 4)
+    for world in (2, 3, 4):
+        tot = np.zeros_like(want)
+        for r in range(world):
+            z0, z1 = slab_planes(50, world, r)
+            tot += u64(sharded_field_bpfd(fd[z0:z1], t, 4))
+        assert (tot == want).all(), world
