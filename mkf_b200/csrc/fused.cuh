@@ -37,7 +37,7 @@ struct FieldTask
    int X, Y, Z, K, D, nSegX, nTileY, nSlabZ;
    long long nItems;
    uint32_t nanRank;
-   int rankHi, complement, variant;  // variant: 0 f32 >, 1 f32 >=, 2 f64 >, 3 f64 >=
+   int rankHi, complement, variant;  // variant: 0 f32 >, 1 f32 >=, 2 f64 >, 3 f64 >=; + 4: shifted edge items
    uint64_t *out;
    int outRow[MKF_MAX_THRESH];
    uint32_t tkey[MKF_MAX_THRESH];

@@ -8,13 +8,17 @@
 // DRAM sectors, half the load bandwidth into the SM); when that word ties with the candidate's or
 // the element is inf/NaN, the element is re-read whole and ranked exactly by binary search.
 //
-// A warp owns 32 x positions (31 cells, neighbouring columns overlap by one element), TY rows and
-// D planes; it walks the planes, keeping per row pair of the previous plane the four corner ranks
-// (one byte each) and their min | max << 8. A cell's pattern for threshold k is all-ones for
-// k < min rank, all-zeros for k >= max rank, and is formed with byte arithmetic on the two faces'
-// packed ranks only for k in between; those codes go to the per-CTA [K][256] shared histogram.
-// All-ones counts are summed per threshold with bit-sliced carry-save adders and all-zeros counts
-// follow from the number of cells, as in fused.cu.
+// A warp owns 32 x positions (31 cells, neighbouring columns overlap by one element), TY row pairs
+// (TY + 1 rows) and D planes; it walks the planes, loading the next plane's TY + 1 words per lane
+// into registers while the current one is ranked and counted, and keeping per row pair of the
+// previous plane the four corner ranks (one byte each) and their min | max << 8. Work items at the
+// field's +x / +y edge are shifted back inside the field (their cells already owned by the
+// neighbouring item are masked), so no load needs a clamp. A cell's pattern for threshold k is
+// all-ones for k < min rank, all-zeros for k >= max rank, and is formed with byte arithmetic on
+// the two faces' packed ranks only for k in between: three predicated slots cover almost every
+// cell, a loop the rest. Codes go to the per-CTA [K][256] shared histogram. All-ones counts are
+// summed per threshold with bit-sliced carry-save adders and all-zeros counts follow from the
+// number of cells, as in fused.cu.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -27,8 +31,9 @@ static constexpr int kThWarps = 8;
 #define THERMO_TY 8
 #endif
 #ifndef THERMO_MINB
-#define THERMO_MINB 3
+#define THERMO_MINB (THERMO_TY == 8 ? 3 : 2)
 #endif
+static constexpr int kThSlots = 3;  // predicated mixed-code slots per cell (K > 1)
 static constexpr int kLutShift = 18;
 static constexpr int kLutSize = 1 << (32 - kLutShift);
 
@@ -51,16 +56,6 @@ __device__ __forceinline__ uint32_t loadWord<double>(const double *__restrict__ 
 {
    return __ldg(reinterpret_cast<const unsigned *>(F) + 2 * i + 1);
 }
-
-// Asynchronous 4-byte global -> shared copy (completes at cp.async.wait_group).
-__device__ __forceinline__ void cpAsync4(uint32_t *dst, const unsigned *src)
-{
-   const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
-   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cpAsyncWait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // Exact rank of the element F[i] by binary search over the sorted thresholds in the field's
 // precision. Kept out of line: it runs only for the rare elements the fast path cannot decide.
@@ -142,15 +137,14 @@ struct ThermoShared
    unsigned long long cells;
 };
 
-template <int TY>
-__device__ __forceinline__ uint32_t *histOf(uint32_t *dyn) { return dyn + kThWarps * 2 * (TY + 1) * 32; }
+// Dynamic shared memory: the [K][256] histogram.
+__host__ __device__ constexpr size_t thermoDynBytes(int K) { return (size_t)K * 256 * sizeof(uint32_t); }
 
 // Load one field's thresholds, build its rank table and clear the histogram (whole CTA).
-template <int TY, typename P>
-__device__ void ctaSetup(const P &a, ThermoShared &S, uint32_t *dyn)
+template <typename P>
+__device__ void ctaSetup(const P &a, ThermoShared &S, uint32_t *hist)
 {
    const int K = a.K;
-   uint32_t *hist = histOf<TY>(dyn);
    for (int i = threadIdx.x; i < K * 256; i += blockDim.x) { hist[i] = 0; }
    for (int i = threadIdx.x; i < 64; i += blockDim.x) {
       S.tlo[i] = a.tlo[i];
@@ -172,12 +166,11 @@ __device__ void ctaSetup(const P &a, ThermoShared &S, uint32_t *dyn)
 
 // Add the CTA's counts of one field to its output rows (whole CTA; call after every warp has
 // added its cells to S.cells): mixed codes as counted, 255 from the all-ones sums, 0 = the rest.
-template <int TY, typename P>
-__device__ void ctaFlush(const P &a, ThermoShared &S, uint32_t *dyn)
+template <typename P>
+__device__ void ctaFlush(const P &a, ThermoShared &S, const uint32_t *hist)
 {
    __syncthreads();
    const int K = a.K;
-   const uint32_t *hist = histOf<TY>(dyn);
    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
    for (int k = warp; k < K; k += kThWarps) {
       uint32_t s = 0;
@@ -203,65 +196,86 @@ __device__ void ctaFlush(const P &a, ThermoShared &S, uint32_t *dyn)
    __syncthreads();
 }
 
-// One warp counts one work item (31 x positions, TY rows, D planes) of the field described by
-// `a` into the CTA's histogram and all-ones totals. Returns the item's number of cells.
-template <typename T, int TY, bool GE, bool SLOT2, typename P>
-__device__ __forceinline__ unsigned long long warpItem(const P &a, long long it, ThermoShared &S, uint32_t *dyn)
+// Gather the top bit of each byte of t, with the top bits of the first word's bytes moved 4 down
+// beforehand (bits 3, 11, 19, 27 and 7, 15, 23, 31), into an 8-bit code: the multiply's shifted
+// partial products never overlap below bit 32.
+__device__ __forceinline__ uint32_t gatherCode(uint32_t t) { return (t * 0x00204081u) >> 24; }
+
+// Add 1 to the shared-memory word at byte address `addr` when `p` holds (predicated, no branch).
+__device__ __forceinline__ void redShared(uint32_t addr, bool p)
 {
+   asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %1, 0;\n\t@q red.shared.add.u32 [%0], 1;\n\t}" ::"r"(addr),
+                "r"((uint32_t)p)
+                : "memory");
+}
+
+// Pattern of a cell for threshold k from its two faces' packed corner ranks R0 (plane z) and R1
+// (plane z + 1), C = 0x7F7F7F7F - k * 0x01010101: adding C sets a byte's top bit iff its rank
+// exceeds k (ranks <= 32, no carries between bytes); the top bits of R0's bytes are moved 4 down,
+// and one multiply gathers all eight (the shifted partial products never overlap below bit 32).
+__device__ __forceinline__ uint32_t cellCode(uint32_t R0, uint32_t R1, uint32_t C)
+{
+   return gatherCode((((R0 + C) >> 4) & 0x08080808u) | ((R1 + C) & 0x80808080u));
+}
+
+// One warp counts one work item (31 x positions, TY row pairs, D planes) of the field described
+// by `a` into the CTA's histogram and all-ones totals. Returns the item's number of cells.
+// INNER: the field has X >= 32, Y > TY, and a positive row stride whose TY multiple fits 32 bits
+// in bytes. NSLOT: 3 mixed-code slots, or 1 for one threshold (a cell then has at most one).
+template <typename T, int TY, bool GE, int NSLOT, bool INNER, typename P>
+__device__ __forceinline__ unsigned long long warpItem(const P &a, long long it, ThermoShared &S, uint32_t *sHist)
+{
+   static_assert(NSLOT == 1 || NSLOT == 3, "one or three slots");
    constexpr int W = sizeof(T) / 4;  // 32-bit words per element; the ranked word is the last one
    const int lane = threadIdx.x & 31;
-   uint32_t *sHist = histOf<TY>(dyn);
-   uint32_t(*stage)[TY + 1][32] = reinterpret_cast<uint32_t(*)[TY + 1][32]>(dyn + (threadIdx.x >> 5) * 2 * (TY + 1) * 32);
    const int K = a.K;
-   const unsigned *__restrict__ F32w = reinterpret_cast<const unsigned *>(a.f) + (W - 1);
-   const long long rowStep = (long long)W * a.sy, planeStep = (long long)W * a.sz;
    const uint32_t nanRank = a.nanRank;
+   const uint32_t hist32 = (uint32_t)__cvta_generic_to_shared(sHist);
 
    const int ix = (int)(it % a.nSegX);
    const long long rest = it / a.nSegX;
    const int iy = (int)(rest % a.nTileY);
    const int iz = (int)(rest / a.nTileY);
-   const int x0 = 31 * ix, y0 = TY * iy, z0 = a.D * iz;
-   const int xl = min(x0 + lane, a.X - 1);  // lanes past the row end re-read the last element
-   const uint32_t vx = ((lane < 31) && (x0 + lane < a.X - 1)) ? 0xFFFFFFFFu : 0u;
-   const int nRow = min(TY, a.Y - 1 - y0);
+   // this item's cells: x in [xs, xe), y in [ys, ye), z in [z0, z0 + nPln)
+   const int xs = 31 * ix, ys = TY * iy, z0 = a.D * iz;
+   const int xe = min(xs + 31, a.X - 1), ye = min(ys + TY, a.Y - 1);
    const int nPln = min(a.D, a.Z - 1 - z0);
-   const int lastRow = a.Y - 1 - y0;  // rows j > lastRow re-read row lastRow
-   const unsigned *__restrict__ P0 = F32w + (long long)W * ((long long)xl * a.sx + (long long)y0 * a.sy + (long long)z0 * a.sz);
-   const unsigned *Pn = P0;
+   // loaded tile: x0 + lane, rows y0 .. y0 + TY (INNER: all inside the field)
+   const int x0 = INNER ? min(xs, a.X - 32) : xs;
+   const int y0 = INNER ? min(ys, a.Y - 1 - TY) : ys;
+   const int xl = INNER ? x0 + lane : min(x0 + lane, a.X - 1);  // clamped: lanes past the row end re-read it
+   const int lastRow = a.Y - 1 - y0;                              // clamped: rows past it re-read it
+   const int jlo = ys - y0, jhi = ye - y0;                        // counted row pairs j in [jlo, jhi)
+   const uint32_t vx = (x0 + lane >= xs && x0 + lane < xe) ? 0xFFFFFFFFu : 0u;
+   const long long rowStep = (long long)W * a.sy, planeStep = (long long)W * a.sz;
+   const uint32_t rowBytes = (uint32_t)(rowStep * 4);
+   const long long e00 = (long long)xl * a.sx + (long long)y0 * a.sy + (long long)z0 * a.sz;
+   const unsigned *__restrict__ Pz = reinterpret_cast<const unsigned *>(a.f) + (W - 1) + (long long)W * e00;
 
-   // stage plane 0; every lane later reads back only the words it copied itself
-   {
-      const unsigned *q = Pn;
+   uint32_t wn[TY + 1];  // the next plane's ranked words
+   auto loadPlane = [&](const unsigned *Pp) {
 #pragma unroll
       for (int j = 0; j <= TY; ++j) {
-         cpAsync4(&stage[0][j][lane], q);
-         if (j < lastRow) { q += rowStep; }
+         if (INNER) {
+            wn[j] = __ldg(reinterpret_cast<const unsigned *>(reinterpret_cast<const char *>(Pp) + (uint64_t)(rowBytes * (uint32_t)j)));
+         } else {
+            wn[j] = __ldg(Pp + (long long)min(j, lastRow) * rowStep);
+         }
       }
-      cpAsyncCommit();
-   }
+   };
+   loadPlane(Pz);
+
    uint32_t sF[TY], sM[TY];  // previous plane: face ranks, min | max << 8 per row pair
    PlaneOnes<TY> ones;
    for (int p = 0; p <= nPln; ++p) {
-      Pn += planeStep;
-      if (p < nPln) {  // stage the next plane while this one is ranked and counted
-         const unsigned *q = Pn;
-#pragma unroll
-         for (int j = 0; j <= TY; ++j) {
-            cpAsync4(&stage[(p + 1) & 1][j][lane], q);
-            if (j < lastRow) { q += rowStep; }
-         }
-         cpAsyncCommit();
-         cpAsyncWait<1>();
-      } else {
-         cpAsyncWait<0>();
-      }
-      const uint32_t(*w)[32] = stage[p & 1];
       uint32_t r[TY + 1];
+#pragma unroll
+      for (int j = 0; j <= TY; ++j) { r[j] = wn[j]; }
+      if (p < nPln) { loadPlane(Pz + (long long)(p + 1) * planeStep); }
       uint32_t slow = 0;  // bit j: element of row j needs the exact rank
 #pragma unroll
       for (int j = 0; j <= TY; ++j) {
-         const uint32_t wj = w[j][lane];
+         const uint32_t wj = r[j];
          const uint32_t key = sortKey(wj);
          const uint32_t r0 = S.lut[key >> kLutShift];
          const uint32_t cand = S.key[r0];
@@ -274,11 +288,11 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
       }
       if (W == 2 && slow) {
          const T *Fe = reinterpret_cast<const T *>(a.f);
-         const long long e0 = (long long)xl * a.sx + (long long)y0 * a.sy + (long long)(z0 + p) * a.sz;
+         const long long e0 = e00 + (long long)p * a.sz;
 #pragma unroll
          for (int j = 0; j <= TY; ++j) {
             if ((slow >> j) & 1u) {
-               r[j] = exactRank<T, GE>(Fe, e0 + (long long)min(j, lastRow) * a.sy, S.tlo, S.thi, K, nanRank);
+               r[j] = exactRank<T, GE>(Fe, e0 + (long long)(INNER ? j : min(j, lastRow)) * a.sy, S.tlo, S.thi, K, nanRank);
             }
          }
       }
@@ -307,39 +321,36 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
          const uint32_t fc = __byte_perm(ePrev, e, 0x5410);
          const uint32_t fmn = min(mnPrev, mn), fmx = max(mxPrev, mx);
          const uint32_t rmin = min(sM[j] & 0xFFu, fmn);
-         const uint32_t vmask = (j < nRow) ? vx : 0u;
-         const uint32_t rmax = vmask ? max(sM[j] >> 8, fmx) : rmin;  // invalid cells: no mixed codes
+         const uint32_t vmask = (j >= jlo && j < jhi) ? vx : 0u;
+         const uint32_t rmax = vmask ? max(sM[j] >> 8, fmx) : rmin;  // uncounted cells: no mixed codes
          ones.add(j, thermo(rmin) & vmask);
          {
-            // codes of the cell for k = rmin and rmin + 1, predicated (no branch); the rare
-            // cells spanning more thresholds finish in a loop
+            // Mixed codes, k = rmin .. rmax - 1. With d = corner rank - rmin per byte, the code
+            // for k = rmin + q marks the corners with d > q; while the spread rmax - rmin is at
+            // most 3, d has two bits, and with lo / hi the masks of corners whose d has bit 0 /
+            // bit 1 set the codes are lo | hi, hi, lo & hi. Wider cells (about 1 in 100) count
+            // all their codes in a loop.
             const uint32_t R0 = sF[j], R1 = fc;
-            const uint32_t C0 = 0x7F7F7F7Fu - rmin * 0x01010101u;
-            uint32_t *h = sHist + (rmin << 8);
-            {
-               const uint32_t t0 = (R0 + C0) & 0x80808080u;
-               const uint32_t t1 = (R1 + C0) & 0x80808080u;
-               const uint32_t c = ((t0 * 0x00204081u) >> 28) | (((t1 * 0x00204081u) >> 24) & 0xF0u);
-               if (rmin < rmax) { atomicAdd(h + c, 1u); }
-            }
-            if (SLOT2) {
-               const uint32_t C1 = C0 - 0x01010101u;
-               const uint32_t t0 = (R0 + C1) & 0x80808080u;
-               const uint32_t t1 = (R1 + C1) & 0x80808080u;
-               const uint32_t c = ((t0 * 0x00204081u) >> 28) | (((t1 * 0x00204081u) >> 24) & 0xF0u);
-               if (rmin + 1 < rmax) { atomicAdd(h + 256 + c, 1u); }
-               if (rmin + 2 < rmax) {
-                  uint32_t C = C1 - 0x01010101u;
-                  uint32_t *hk = h + 512;
-                  uint32_t k = rmin + 2;
-                  do {
-                     const uint32_t u0 = (R0 + C) & 0x80808080u;
-                     const uint32_t u1 = (R1 + C) & 0x80808080u;
-                     const uint32_t cc = ((u0 * 0x00204081u) >> 28) | (((u1 * 0x00204081u) >> 24) & 0xF0u);
-                     atomicAdd(hk + cc, 1u);
+            const uint32_t spread = rmax - rmin;
+            const uint32_t rowAddr = hist32 + (rmin << 10);
+            const uint32_t rb = rmin * 0x01010101u;
+            const uint32_t D0 = R0 - rb, D1 = R1 - rb;
+            const uint32_t lo = gatherCode(((D0 << 3) & 0x08080808u) | ((D1 << 7) & 0x80808080u));
+            if (NSLOT == 1) {
+               redShared(rowAddr + (lo << 2), spread != 0);
+            } else {
+               const uint32_t hi = gatherCode(((D0 << 2) & 0x08080808u) | ((D1 << 6) & 0x80808080u));
+               const bool fast = spread < 4;
+               redShared(rowAddr + ((lo | hi) << 2), fast && spread > 0);
+               redShared(rowAddr + 1024 + (hi << 2), fast && spread > 1);
+               redShared(rowAddr + 2048 + ((lo & hi) << 2), fast && spread > 2);
+               if (!fast) {
+                  uint32_t C = 0x7F7F7F7Fu - rb, addr = rowAddr;
+                  for (uint32_t k = rmin; k < rmax; ++k) {
+                     redShared(addr + (cellCode(R0, R1, C) << 2), true);
                      C -= 0x01010101u;
-                     hk += 256;
-                  } while (++k < rmax);
+                     addr += 1024;
+                  }
                }
             }
          }
@@ -354,21 +365,21 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
       const uint32_t s = __reduce_add_sync(FULL, ones.total(k));
       if (lane == 0 && s) { atomicAdd(&S.ones[k], s); }
    }
-   return (unsigned long long)max(0, min(31, a.X - 1 - x0)) * (unsigned)nRow * (unsigned)nPln;
+   return (unsigned long long)(xe - xs) * (unsigned)(jhi - jlo) * (unsigned)nPln;
 }
 
-template <typename T, int TY, bool GE, bool SLOT2>
-__global__ void __launch_bounds__(kThWarps * 32, TY == 8 ? THERMO_MINB : 2) thermoBPFD(const __grid_constant__ FusedArgs a)
+template <typename T, int TY, bool GE, int NSLOT, bool INNER>
+__global__ void __launch_bounds__(kThWarps * 32, THERMO_MINB) thermoBPFD(const __grid_constant__ FusedArgs a)
 {
    __shared__ ThermoShared S;
-   extern __shared__ uint32_t sDyn[];
-   ctaSetup<TY>(a, S, sDyn);
+   extern __shared__ uint32_t sHist[];
+   ctaSetup(a, S, sHist);
    const long long gw = (long long)blockIdx.x * kThWarps + (threadIdx.x >> 5);
    const long long nw = (long long)gridDim.x * kThWarps;
    unsigned long long cells = 0;
-   for (long long it = gw; it < a.nItems; it += nw) { cells += warpItem<T, TY, GE, SLOT2>(a, it, S, sDyn); }
+   for (long long it = gw; it < a.nItems; it += nw) { cells += warpItem<T, TY, GE, NSLOT, INNER>(a, it, S, sHist); }
    if ((threadIdx.x & 31) == 0 && cells) { atomicAdd(&S.cells, cells); }
-   ctaFlush<TY>(a, S, sDyn);
+   ctaFlush(a, S, sHist);
 }
 
 // ---------------------------------------------------------------- many fields, one launch
@@ -382,7 +393,7 @@ __global__ void __launch_bounds__(kThWarps * 32, THERMO_MINB) thermoBatch(const 
    __shared__ ThermoShared S;
    __shared__ FieldTask F;
    __shared__ int sChunk;
-   extern __shared__ uint32_t sDyn[];
+   extern __shared__ uint32_t sHist[];
    int cur = -1;
    unsigned long long cells = 0;
    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -397,28 +408,32 @@ __global__ void __launch_bounds__(kThWarps * 32, THERMO_MINB) thermoBatch(const 
          if (cur >= 0) {
             if (lane == 0 && cells) { atomicAdd(&S.cells, cells); }
             cells = 0;
-            ctaFlush<TY>(F, S, sDyn);
+            ctaFlush(F, S, sHist);
          }
          const uint32_t *src = reinterpret_cast<const uint32_t *>(b.tasks + ch.field);
          for (int i = threadIdx.x; i < (int)(sizeof(FieldTask) / 4); i += blockDim.x) {
             reinterpret_cast<uint32_t *>(&F)[i] = src[i];
          }
          __syncthreads();
-         ctaSetup<TY>(F, S, sDyn);
+         ctaSetup(F, S, sHist);
          cur = ch.field;
       }
       for (long long it = ch.begin + warp; it < ch.end; it += kThWarps) {
          switch (F.variant) {
-            case 0: cells += warpItem<float, TY, false, true>(F, it, S, sDyn); break;
-            case 1: cells += warpItem<float, TY, true, true>(F, it, S, sDyn); break;
-            case 2: cells += warpItem<double, TY, false, true>(F, it, S, sDyn); break;
-            default: cells += warpItem<double, TY, true, true>(F, it, S, sDyn); break;
+            case 0: cells += warpItem<float, TY, false, kThSlots, false>(F, it, S, sHist); break;
+            case 1: cells += warpItem<float, TY, true, kThSlots, false>(F, it, S, sHist); break;
+            case 2: cells += warpItem<double, TY, false, kThSlots, false>(F, it, S, sHist); break;
+            case 3: cells += warpItem<double, TY, true, kThSlots, false>(F, it, S, sHist); break;
+            case 4: cells += warpItem<float, TY, false, kThSlots, true>(F, it, S, sHist); break;
+            case 5: cells += warpItem<float, TY, true, kThSlots, true>(F, it, S, sHist); break;
+            case 6: cells += warpItem<double, TY, false, kThSlots, true>(F, it, S, sHist); break;
+            default: cells += warpItem<double, TY, true, kThSlots, true>(F, it, S, sHist); break;
          }
       }
    }
    if (cur >= 0) {
       if (lane == 0 && cells) { atomicAdd(&S.cells, cells); }
-      ctaFlush<TY>(F, S, sDyn);
+      ctaFlush(F, S, sHist);
    }
 }
 
@@ -440,26 +455,32 @@ static uint32_t thresholdKey(double t, int enc, bool ge)
    return sortKey(u);
 }
 
-template <typename T, int TY, bool GE, bool SLOT2>
+template <typename T, int TY, bool GE, int NSLOT, bool INNER>
 static int launchThermoT(const FusedArgs &a, cudaStream_t s)
 {
    static int blocksPerSM = -1;
-   auto kern = thermoBPFD<T, TY, GE, SLOT2>;
-   const size_t stageBytes = (size_t)kThWarps * 2 * (TY + 1) * 32 * sizeof(uint32_t);
-   const size_t smem = stageBytes + (size_t)a.K * 256 * sizeof(uint32_t);
+   auto kern = thermoBPFD<T, TY, GE, NSLOT, INNER>;
    if (blocksPerSM < 0) {
-      const size_t maxSmem = stageBytes + (size_t)MKF_MAX_THRESH * 256 * 4;
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)maxSmem);
+      // static + dynamic shared memory exceeds the default 48 KB for K > 23
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)thermoDynBytes(MKF_MAX_THRESH));
       int n = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, kThWarps * 32, maxSmem);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, kThWarps * 32, thermoDynBytes(MKF_MAX_THRESH));
       blocksPerSM = n > 0 ? n : 1;
    }
    long long grid = (a.nItems + kThWarps - 1) / kThWarps;
    const long long cap = (long long)smCount() * blocksPerSM;
    if (grid > cap) { grid = cap; }
    if (grid < 1) { grid = 1; }
-   kern<<<(unsigned)grid, kThWarps * 32, smem, s>>>(a);
+   kern<<<(unsigned)grid, kThWarps * 32, thermoDynBytes(a.K), s>>>(a);
    return cudaFail(cudaGetLastError(), "thermoBPFD launch");
+}
+
+// Whether a field's work items can all be shifted inside it (see warpItem's INNER).
+template <typename P>
+static bool innerTiles(const P &a, int enc)
+{
+   const int64_t rowBytes = a.sy * (enc == ENC_F32 ? 4 : 8);
+   return a.X >= 32 && a.Y > THERMO_TY && rowBytes > 0 && rowBytes * THERMO_TY < ((int64_t)1 << 32);
 }
 
 // Fill the key table of a thermometer pass; returns false when two thresholds share a bucket of
@@ -489,7 +510,7 @@ static void itemGrid(P &a, int D)
 
 bool prepareThermoTask(FieldTask &t, int enc)
 {
-   t.variant = (enc == ENC_F32 ? 0 : 2) + (t.rankHi ? 1 : 0);
+   t.variant = (enc == ENC_F32 ? 0 : 2) + (t.rankHi ? 1 : 0) + (innerTiles(t, enc) ? 4 : 0);
    if (!prepareKeys(t, enc)) { return false; }
    itemGrid(t, 32);
    return true;
@@ -500,8 +521,7 @@ int launchThermoBatch(const BatchArgs &b, cudaStream_t s)
    constexpr int TY = THERMO_TY;
    static int blocksPerSM = -1;
    auto kern = thermoBatch<TY>;
-   const size_t stageBytes = (size_t)kThWarps * 2 * (TY + 1) * 32 * sizeof(uint32_t);
-   const size_t smem = stageBytes + (size_t)MKF_MAX_THRESH * 256 * 4;
+   const size_t smem = thermoDynBytes(MKF_MAX_THRESH);
    if (blocksPerSM < 0) {
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       int n = 0;
@@ -515,20 +535,23 @@ int launchThermoBatch(const BatchArgs &b, cudaStream_t s)
    return cudaFail(cudaGetLastError(), "thermoBatch launch");
 }
 
+template <typename T, bool GE>
+static int launchThermoG(const FusedArgs &a, bool inner, cudaStream_t s)
+{
+   constexpr int TY = THERMO_TY;
+   // one threshold: a cell has at most one mixed code
+   if (a.K == 1) { return inner ? launchThermoT<T, TY, GE, 1, true>(a, s) : launchThermoT<T, TY, GE, 1, false>(a, s); }
+   return inner ? launchThermoT<T, TY, GE, kThSlots, true>(a, s) : launchThermoT<T, TY, GE, kThSlots, false>(a, s);
+}
+
 int launchThermo(FusedArgs &a, int enc, cudaStream_t s)
 {
    a.lutOk = prepareKeys(a, enc) ? 1 : 0;
    if (!a.lutOk) { return MKF_ERR_UNSUPPORTED; }
-   constexpr int TY = THERMO_TY;
    itemGrid(a, 32);
-   const bool ge = a.rankHi != 0;
-   // one threshold: a cell has at most one mixed code
-   if (a.K == 1) {
-      if (enc == ENC_F32) { return ge ? launchThermoT<float, TY, true, false>(a, s) : launchThermoT<float, TY, false, false>(a, s); }
-      return ge ? launchThermoT<double, TY, true, false>(a, s) : launchThermoT<double, TY, false, false>(a, s);
-   }
-   if (enc == ENC_F32) { return ge ? launchThermoT<float, TY, true, true>(a, s) : launchThermoT<float, TY, false, true>(a, s); }
-   return ge ? launchThermoT<double, TY, true, true>(a, s) : launchThermoT<double, TY, false, true>(a, s);
+   const bool ge = a.rankHi != 0, inner = innerTiles(a, enc);
+   if (enc == ENC_F32) { return ge ? launchThermoG<float, true>(a, inner, s) : launchThermoG<float, false>(a, inner, s); }
+   return ge ? launchThermoG<double, true>(a, inner, s) : launchThermoG<double, false>(a, inner, s);
 }
 
 }  // namespace mkf
