@@ -137,15 +137,21 @@ struct ThermoShared
    unsigned long long cells;
 };
 
-// Dynamic shared memory: the [K][256] histogram.
-__host__ __device__ constexpr size_t thermoDynBytes(int K) { return (size_t)K * 256 * sizeof(uint32_t); }
+// Dynamic shared memory: the [K][256] histogram, rows kHistRow words apart (one word of skew, so
+// that equal codes of different thresholds fall in different banks), then one scratch word per
+// lane.
+#ifndef THERMO_HROW
+#define THERMO_HROW 257
+#endif
+static constexpr int kHistRow = THERMO_HROW;
+__host__ __device__ constexpr size_t thermoDynBytes(int K) { return ((size_t)K * kHistRow + 32) * sizeof(uint32_t); }
 
 // Load one field's thresholds, build its rank table and clear the histogram (whole CTA).
 template <typename P>
 __device__ void ctaSetup(const P &a, ThermoShared &S, uint32_t *hist)
 {
    const int K = a.K;
-   for (int i = threadIdx.x; i < K * 256; i += blockDim.x) { hist[i] = 0; }
+   for (int i = threadIdx.x; i < K * kHistRow; i += blockDim.x) { hist[i] = 0; }
    for (int i = threadIdx.x; i < 64; i += blockDim.x) {
       S.tlo[i] = a.tlo[i];
       S.thi[i] = a.thi[i];
@@ -174,7 +180,7 @@ __device__ void ctaFlush(const P &a, ThermoShared &S, const uint32_t *hist)
    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
    for (int k = warp; k < K; k += kThWarps) {
       uint32_t s = 0;
-      for (int c = 1 + lane; c < 255; c += 32) { s += hist[k * 256 + c]; }
+      for (int c = 1 + lane; c < 255; c += 32) { s += hist[k * kHistRow + c]; }
       s = __reduce_add_sync(FULL, s);
       if (lane == 0) {
          const unsigned long long n1 = S.ones[k];
@@ -187,7 +193,7 @@ __device__ void ctaFlush(const P &a, ThermoShared &S, const uint32_t *hist)
    }
    for (int i = threadIdx.x; i < K * 256; i += blockDim.x) {
       const int c = i & 255;
-      const uint32_t v = hist[i];
+      const uint32_t v = hist[(i >> 8) * kHistRow + c];
       if (v && c != 0 && c != 255) {
          const int cc = a.complement ? 255 - c : c;
          atomicAdd((unsigned long long *)(a.out + (size_t)a.outRow[i >> 8] * 256 + cc), (unsigned long long)v);
@@ -201,12 +207,11 @@ __device__ void ctaFlush(const P &a, ThermoShared &S, const uint32_t *hist)
 // partial products never overlap below bit 32.
 __device__ __forceinline__ uint32_t gatherCode(uint32_t t) { return (t * 0x00204081u) >> 24; }
 
-// Add 1 to the shared-memory word at byte address `addr` when `p` holds (predicated, no branch).
-__device__ __forceinline__ void redShared(uint32_t addr, bool p)
+// Add 1 to the shared-memory word at byte address `addr` (a predicated atomic costs a branch, so
+// slots with nothing to count add to a per-lane scratch word instead).
+__device__ __forceinline__ void redShared(uint32_t addr)
 {
-   asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %1, 0;\n\t@q red.shared.add.u32 [%0], 1;\n\t}" ::"r"(addr),
-                "r"((uint32_t)p)
-                : "memory");
+   asm volatile("red.shared.add.u32 [%0], 1;" ::"r"(addr) : "memory");
 }
 
 // Pattern of a cell for threshold k from its two faces' packed corner ranks R0 (plane z) and R1
@@ -231,6 +236,7 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
    const int K = a.K;
    const uint32_t nanRank = a.nanRank;
    const uint32_t hist32 = (uint32_t)__cvta_generic_to_shared(sHist);
+   const uint32_t trash = hist32 + (uint32_t)(K * kHistRow + lane) * 4u;
 
    const int ix = (int)(it % a.nSegX);
    const long long rest = it / a.nSegX;
@@ -272,7 +278,7 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
 #pragma unroll
       for (int j = 0; j <= TY; ++j) { r[j] = wn[j]; }
       if (p < nPln) { loadPlane(Pz + (long long)(p + 1) * planeStep); }
-      uint32_t slow = 0;  // bit j: element of row j needs the exact rank
+      bool slow = false;  // some element of this lane's column needs the exact rank
 #pragma unroll
       for (int j = 0; j <= TY; ++j) {
          const uint32_t wj = r[j];
@@ -281,7 +287,7 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
          const uint32_t cand = S.key[r0];
          r[j] = r0 + (GE ? (key >= cand) : (key > cand));
          if (W == 2) {
-            slow |= (uint32_t)((key == cand) | ((key - 0x00100000u) >= 0xFFE00000u)) << j;
+            slow = slow || key == cand || key >= 0xFFF00000u || key < 0x00100000u;
          } else {
             r[j] = ((wj & 0x7FFFFFFFu) > 0x7F800000u) ? nanRank : r[j];
          }
@@ -291,9 +297,7 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
          const long long e0 = e00 + (long long)p * a.sz;
 #pragma unroll
          for (int j = 0; j <= TY; ++j) {
-            if ((slow >> j) & 1u) {
-               r[j] = exactRank<T, GE>(Fe, e0 + (long long)(INNER ? j : min(j, lastRow)) * a.sy, S.tlo, S.thi, K, nanRank);
-            }
+            r[j] = exactRank<T, GE>(Fe, e0 + (long long)(INNER ? j : min(j, lastRow)) * a.sy, S.tlo, S.thi, K, nanRank);
          }
       }
       uint32_t rR = __shfl_down_sync(FULL, r[0], 1);
@@ -326,30 +330,40 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
          ones.add(j, thermo(rmin) & vmask);
          {
             // Mixed codes, k = rmin .. rmax - 1. With d = corner rank - rmin per byte, the code
-            // for k = rmin + q marks the corners with d > q; while the spread rmax - rmin is at
-            // most 3, d has two bits, and with lo / hi the masks of corners whose d has bit 0 /
-            // bit 1 set the codes are lo | hi, hi, lo & hi. Wider cells (about 1 in 100) count
-            // all their codes in a loop.
+            // for k = rmin + q marks the corners with d > q; with b0, b1, b2 the masks of corners
+            // whose d has bit 0, 1, 2 set, the codes for a spread rmax - rmin up to 3 are
+            // b0 | b1, b1, b0 & b1, and up to 7 (about 1 cell in 100) seven formulas in b0..b2.
+            // Wider cells count their codes one threshold at a time.
             const uint32_t R0 = sF[j], R1 = fc;
             const uint32_t spread = rmax - rmin;
-            const uint32_t rowAddr = hist32 + (rmin << 10);
+            const uint32_t rowAddr = hist32 + rmin * (kHistRow * 4);
             const uint32_t rb = rmin * 0x01010101u;
             const uint32_t D0 = R0 - rb, D1 = R1 - rb;
-            const uint32_t lo = gatherCode(((D0 << 3) & 0x08080808u) | ((D1 << 7) & 0x80808080u));
+            const uint32_t b0 = gatherCode(((D0 << 3) & 0x08080808u) | ((D1 << 7) & 0x80808080u));
             if (NSLOT == 1) {
-               redShared(rowAddr + (lo << 2), spread != 0);
+               redShared(spread != 0 ? rowAddr + (b0 << 2) : trash);
             } else {
-               const uint32_t hi = gatherCode(((D0 << 2) & 0x08080808u) | ((D1 << 6) & 0x80808080u));
+               const uint32_t b1 = gatherCode(((D0 << 2) & 0x08080808u) | ((D1 << 6) & 0x80808080u));
                const bool fast = spread < 4;
-               redShared(rowAddr + ((lo | hi) << 2), fast && spread > 0);
-               redShared(rowAddr + 1024 + (hi << 2), fast && spread > 1);
-               redShared(rowAddr + 2048 + ((lo & hi) << 2), fast && spread > 2);
+               redShared(fast && spread > 0 ? rowAddr + ((b0 | b1) << 2) : trash);
+               redShared(fast && spread > 1 ? rowAddr + kHistRow * 4 + (b1 << 2) : trash);
+               redShared(fast && spread > 2 ? rowAddr + kHistRow * 8 + ((b0 & b1) << 2) : trash);
                if (!fast) {
-                  uint32_t C = 0x7F7F7F7Fu - rb, addr = rowAddr;
-                  for (uint32_t k = rmin; k < rmax; ++k) {
-                     redShared(addr + (cellCode(R0, R1, C) << 2), true);
-                     C -= 0x01010101u;
-                     addr += 1024;
+                  if (spread < 8) {
+                     const uint32_t b2 = gatherCode(((D0 << 1) & 0x08080808u) | ((D1 << 5) & 0x80808080u));
+                     const uint32_t c[7] = {b0 | b1 | b2, b1 | b2,      b2 | (b1 & b0), b2,
+                                            b2 & (b1 | b0), b2 & b1, b2 & b1 & b0};
+#pragma unroll
+                     for (int q = 0; q < 7; ++q) {
+                        redShared((uint32_t)q < spread ? rowAddr + q * (kHistRow * 4) + (c[q] << 2) : trash);
+                     }
+                  } else {
+                     uint32_t C = 0x7F7F7F7Fu - rb, addr = rowAddr;
+                     for (uint32_t k = rmin; k < rmax; ++k) {
+                        redShared(addr + (cellCode(R0, R1, C) << 2));
+                        C -= 0x01010101u;
+                        addr += kHistRow * 4;
+                     }
                   }
                }
             }
