@@ -89,10 +89,13 @@ struct MKFBatchPlan
 {
    uint64_t *out = nullptr;
    size_t rows = 0;
-   FieldTask *dTasks = nullptr;
+   FieldTask *dTasks = nullptr;     // thermometer-kernel fields
    BatchChunk *dChunks = nullptr;
-   unsigned *dCounter = nullptr;
    int nChunks = 0;
+   WordTask *dWTasks[2] = {nullptr, nullptr};  // word-kernel fields, FP32 and FP64
+   BatchChunk *dWChunks[2] = {nullptr, nullptr};
+   int nWChunks[2] = {0, 0};
+   unsigned *dCounter = nullptr;    // chunk counters: thermometer, words FP32, words FP64
    std::vector<ConstEntry> consts;
    std::vector<unsigned long long> constCells;
    struct Fallback
@@ -118,6 +121,10 @@ static void freePlan(MKFBatchPlan *p)
    if (p->graph) { cudaGraphDestroy(p->graph); }
    if (p->dTasks) { cudaFree(p->dTasks); }
    if (p->dChunks) { cudaFree(p->dChunks); }
+   for (int e = 0; e < 2; e++) {
+      if (p->dWTasks[e]) { cudaFree(p->dWTasks[e]); }
+      if (p->dWChunks[e]) { cudaFree(p->dWChunks[e]); }
+   }
    if (p->dCounter) { cudaFree(p->dCounter); }
    delete p;
 }
@@ -130,6 +137,8 @@ MKF_API int mkfBatchPlanCreate(MKFBatchPlan **pp, uint64_t *pBPFD, const MKFFiel
    p->out = pBPFD;
    std::vector<FieldTask> tasks;
    std::vector<BatchChunk> chunks;
+   std::vector<WordTask> wtasks[2];
+   std::vector<BatchChunk> wchunks[2];
    size_t row = 0;
    for (int i = 0; i < nF; i++) {
       const MKFFieldDesc *d = pF + i;
@@ -143,10 +152,19 @@ MKF_API int mkfBatchPlanCreate(MKFBatchPlan **pp, uint64_t *pBPFD, const MKFFiel
       const unsigned long long cells = (unsigned long long)(d->def[0] - 1) * (d->def[1] - 1) * (d->def[2] - 1);
       const size_t c0 = p->consts.size();
       FieldTask t;
+      WordTask w;
       bool varying = false;
-      const bool ok = planBatchField(d, ts, (int)row, t, p->consts, varying);
+      const int kind = planBatchField(d, ts, (int)row, t, w, p->consts, varying);
       for (size_t c = c0; c < p->consts.size(); c++) { p->constCells.push_back(cells); }
-      if (cells > 0 && ok) {
+      if (cells > 0 && kind == kPlanWords) {
+         const int e = d->enc == ENC_F32 ? 0 : 1;
+         const int f = (int)wtasks[e].size();
+         for (long long b = 0; b < w.nItems; b += kChunkItems) {
+            wchunks[e].push_back({f, 0, b, std::min<long long>(b + kChunkItems, w.nItems)});
+         }
+         w.out = pBPFD;
+         wtasks[e].push_back(w);
+      } else if (cells > 0 && kind == kPlanThermo) {
          const int f = (int)tasks.size();
          for (long long b = 0; b < t.nItems; b += kChunkItems) {
             chunks.push_back({f, 0, b, std::min<long long>(b + kChunkItems, t.nItems)});
@@ -169,14 +187,21 @@ MKF_API int mkfBatchPlanCreate(MKFBatchPlan **pp, uint64_t *pBPFD, const MKFFiel
       row += (size_t)ts->nT;
    }
    p->rows = row;
-   cudaError_t e = cudaSuccess;
-   if (!tasks.empty()) {
+   cudaError_t e = cudaMalloc(&p->dCounter, 3 * sizeof(unsigned));
+   if (e == cudaSuccess && !tasks.empty()) {
       e = cudaMalloc(&p->dTasks, tasks.size() * sizeof(FieldTask));
       if (e == cudaSuccess) { e = cudaMalloc(&p->dChunks, chunks.size() * sizeof(BatchChunk)); }
-      if (e == cudaSuccess) { e = cudaMalloc(&p->dCounter, sizeof(unsigned)); }
       if (e == cudaSuccess) { e = cudaMemcpy(p->dTasks, tasks.data(), tasks.size() * sizeof(FieldTask), cudaMemcpyHostToDevice); }
       if (e == cudaSuccess) { e = cudaMemcpy(p->dChunks, chunks.data(), chunks.size() * sizeof(BatchChunk), cudaMemcpyHostToDevice); }
       p->nChunks = (int)chunks.size();
+   }
+   for (int k = 0; k < 2 && e == cudaSuccess; k++) {
+      if (wtasks[k].empty()) { continue; }
+      e = cudaMalloc(&p->dWTasks[k], wtasks[k].size() * sizeof(WordTask));
+      if (e == cudaSuccess) { e = cudaMalloc(&p->dWChunks[k], wchunks[k].size() * sizeof(BatchChunk)); }
+      if (e == cudaSuccess) { e = cudaMemcpy(p->dWTasks[k], wtasks[k].data(), wtasks[k].size() * sizeof(WordTask), cudaMemcpyHostToDevice); }
+      if (e == cudaSuccess) { e = cudaMemcpy(p->dWChunks[k], wchunks[k].data(), wchunks[k].size() * sizeof(BatchChunk), cudaMemcpyHostToDevice); }
+      p->nWChunks[k] = (int)wchunks[k].size();
    }
    if (e != cudaSuccess) {
       freePlan(p);
@@ -195,9 +220,20 @@ static int planLaunchOn(MKFBatchPlan *p, cudaStream_t s)
    for (size_t i = 0; i < p->consts.size() && rc == MKF_OK; i++) {
       rc = launchConstBin(p->out, p->consts[i].row, p->consts[i].bin, p->constCells[i], s);
    }
-   if (rc == MKF_OK && p->nChunks > 0) {
-      e = cudaMemsetAsync(p->dCounter, 0, sizeof(unsigned), s);
+   if (rc == MKF_OK && (p->nChunks > 0 || p->nWChunks[0] > 0 || p->nWChunks[1] > 0)) {
+      e = cudaMemsetAsync(p->dCounter, 0, 3 * sizeof(unsigned), s);
       if (e != cudaSuccess) { return cudaFail(e, "batch counter clear"); }
+   }
+   for (int k = 0; k < 2 && rc == MKF_OK; k++) {
+      if (p->nWChunks[k] == 0) { continue; }
+      WordBatchArgs w;
+      w.tasks = p->dWTasks[k];
+      w.chunks = p->dWChunks[k];
+      w.nChunks = p->nWChunks[k];
+      w.counter = p->dCounter + 1 + k;
+      rc = launchWordsBatch(w, k == 0 ? ENC_F32 : ENC_F64, s);
+   }
+   if (rc == MKF_OK && p->nChunks > 0) {
       BatchArgs b;
       b.tasks = p->dTasks;
       b.chunks = p->dChunks;

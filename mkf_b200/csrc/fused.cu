@@ -334,13 +334,15 @@ int launchConstBin(uint64_t *out, int row, int bin, unsigned long long cells, cu
 
 void floatBoundsPlain(double t, double &tlo, double &thi) { floatBounds(t, tlo, thi); }
 
-// Split one field of a batch: constant maps go to `consts` (rows offset by rowBase); if every other
-// threshold shares one thermometer relation and the thresholds fit the rank table, `t` is filled
-// for the batched kernel and true is returned; otherwise the field takes the single-field path.
-bool planBatchField(const MKFFieldDesc *pF, const MKFThreshSet *pT, int rowBase, FieldTask &t, std::vector<ConstEntry> &consts,
-                    bool &anyVarying)
+// Split one field of a batch: constant maps go to `consts` (rows offset by rowBase). One or two
+// other thresholds fill `w` for the batched word kernel (returns kPlanWords); more thresholds that
+// share one thermometer relation and fit the rank table fill `t` for the batched thermometer
+// kernel (kPlanThermo); otherwise the field takes the single-field path (kPlanSingle).
+int planBatchField(const MKFFieldDesc *pF, const MKFThreshSet *pT, int rowBase, FieldTask &t, WordTask &w,
+                   std::vector<ConstEntry> &consts, bool &anyVarying)
 {
    memset(&t, 0, sizeof(t));
+   memset(&w, 0, sizeof(w));
    const int K = pT->nT;
    int idx[MKF_MAX_THRESH], n = 0, cls0 = -2;
    for (int i = 0; i < K; i++) {
@@ -361,10 +363,28 @@ bool planBatchField(const MKFFieldDesc *pF, const MKFThreshSet *pT, int rowBase,
       idx[n++] = i;
    }
    anyVarying = n > 0;
-   if (n == 0 || cls0 < 0) { return false; }
-   std::stable_sort(idx, idx + n, [&](int x, int y) { return pT->t[x] < pT->t[y]; });
+   if (n == 0) { return kPlanSingle; }
    const int X = pF->def[0], Y = pF->def[1], Z = pF->def[2];
    const bool planar = !(pF->stride[0] | pF->stride[1] | pF->stride[2]);
+   if (n <= 2) {
+      w.f = pF->p;
+      w.sx = planar ? 1 : pF->stride[0];
+      w.sy = planar ? (int64_t)X : pF->stride[1];
+      w.sz = planar ? (int64_t)X * Y : pF->stride[2];
+      w.X = X; w.Y = Y; w.Z = Z;
+      w.K = n;
+      for (int k = 0; k < n; k++) {
+         const double tv = pT->t[idx[k]];
+         if (pF->enc == ENC_F32) { floatBounds(tv, w.tlo[k], w.thi[k]); }
+         else { w.tlo[k] = w.thi[k] = tv; }
+         w.m[k] = (pT->m ? pT->m[idx[k]] : pT->mAll) & BMC_AL;
+         w.outRow[k] = rowBase + idx[k];
+      }
+      prepareWordTask(w, pF->enc);
+      return kPlanWords;
+   }
+   if (cls0 < 0) { return kPlanSingle; }
+   std::stable_sort(idx, idx + n, [&](int x, int y) { return pT->t[x] < pT->t[y]; });
    t.f = pF->p;
    t.sx = planar ? 1 : pF->stride[0];
    t.sy = planar ? (int64_t)X : pF->stride[1];
@@ -382,7 +402,7 @@ bool planBatchField(const MKFFieldDesc *pF, const MKFThreshSet *pT, int rowBase,
    t.complement = (cls0 >= 2);
    const bool eqBit = (cls0 == 1 || cls0 == 3);
    t.nanRank = (eqBit != (t.complement != 0)) ? (uint32_t)n : 0u;
-   return prepareThermoTask(t, pF->enc);
+   return prepareThermoTask(t, pF->enc) ? kPlanThermo : kPlanSingle;
 }
 
 int fieldBPFD(uint64_t *out, const MKFFieldDesc *pF, const MKFThreshSet *pT, int flags, cudaStream_t s,

@@ -44,6 +44,24 @@ struct FieldTask
    double tlo[64], thi[64];
 };
 
+// One field for the word-parallel kernels (one or two thresholds of any relation).
+struct WordTask
+{
+   const void *f;
+   int64_t sx, sy, sz;    // element strides
+   int X, Y, Z;
+   int K;                 // 1 or 2
+   int cls[2];            // relation class per threshold (words.cu)
+   uint32_t m[2];         // relation masks
+   double tlo[2], thi[2]; // exact-equivalent thresholds for "f > t" / "f >= t" tests
+   int outRow[2];
+   int complement;        // the map is counted negated: code c is stored in bin 255 - c
+   int variant;           // batched kernel: which instantiation counts this field
+   uint64_t *out;
+   int nChunkX, nTileY, nSlabZ;
+   long long nItems;
+};
+
 // Consecutive work items [begin, end) of one field.
 struct BatchChunk
 {
@@ -59,13 +77,27 @@ struct BatchArgs
    unsigned *counter;  // next chunk to hand out; zero at launch
 };
 
+struct WordBatchArgs
+{
+   const WordTask *tasks;
+   const BatchChunk *chunks;
+   int nChunks;
+   unsigned *counter;  // next chunk to hand out; zero at launch
+};
+
 struct ConstEntry { int row, bin; };
-bool planBatchField(const MKFFieldDesc *pF, const MKFThreshSet *pT, int rowBase, FieldTask &t, std::vector<ConstEntry> &consts,
-                    bool &anyVarying);
+enum { kPlanSingle = 0, kPlanThermo = 1, kPlanWords = 2 };
+int planBatchField(const MKFFieldDesc *pF, const MKFThreshSet *pT, int rowBase, FieldTask &t, WordTask &w,
+                   std::vector<ConstEntry> &consts, bool &anyVarying);
 
 // Fill a task's key table and item grid; false if its thresholds share a rank-table bucket.
 bool prepareThermoTask(FieldTask &t, int enc);
 int launchThermoBatch(const BatchArgs &b, cudaStream_t s);
+
+// Fill a word task's relation classes, batched variant and item grid (words.cu); launch the
+// batched word kernel over the chunks of tasks of one element type.
+void prepareWordTask(WordTask &a, int enc);
+int launchWordsBatch(const WordBatchArgs &b, int enc, cudaStream_t s);
 
 // Word-parallel kernel for one or two thresholds of any relations (words.cu); `masks` are the
 // relation masks of f's (sorted) thresholds. MKF_ERR_UNSUPPORTED for other K.

@@ -27,21 +27,6 @@ static constexpr int kWdD = 32;
 // Relation class of a threshold: every class is one comparison (NaN maps as the EQ bit says).
 enum WordCls { kGT = 0, kGE = 1, kLT = 2, kLE = 3, kGEN = 4 };
 
-struct WordArgs
-{
-   const void *f;
-   int64_t sx, sy, sz;
-   int X, Y, Z;
-   int K;                 // 1 or 2
-   int cls[2];
-   uint32_t m[2];         // relation masks (GEN)
-   double tlo[2], thi[2]; // exact-equivalent thresholds for "f > t" / "f >= t" tests
-   int outRow[2];
-   uint64_t *out;
-   int nChunkX, nTileY, nSlabZ;
-   long long nItems;
-};
-
 template <typename T>
 __device__ __forceinline__ uint32_t mapBit(T v, int cls, uint32_t m, T tlo, T thi)
 {
@@ -85,7 +70,7 @@ __device__ __forceinline__ void loadPlane(T (&v)[32], const T *__restrict__ p, i
 // Map, pack and count one plane (see the file comment). `first`: no previous plane yet.
 // `sRow` is the warp's 32-word transposition buffer per threshold.
 template <typename T, int KMAX, int CLS0, int CLS1>
-__device__ __forceinline__ void countPlane(const T (&v)[32], WordCarry<KMAX> &c, const WordArgs &a, const T *tlo,
+__device__ __forceinline__ void countPlane(const T (&v)[32], WordCarry<KMAX> &c, const uint32_t *m, const T *tlo,
                                            const T *thi, bool xin, int lane, uint32_t vm, bool first,
                                            uint32_t (*sRow)[32], uint32_t *sHist)
 {
@@ -95,7 +80,7 @@ __device__ __forceinline__ void countPlane(const T (&v)[32], WordCarry<KMAX> &c,
       for (int k = 0; k < KMAX; k++) {
          const int cls = k == 0 ? CLS0 : CLS1;
          // every lane stores the same (warp-uniform) word
-         sRow[k][r] = __ballot_sync(FULL, xin && mapBit<T>(v[r], cls, a.m[k], tlo[k], thi[k]));
+         sRow[k][r] = __ballot_sync(FULL, xin && mapBit<T>(v[r], cls, m[k], tlo[k], thi[k]));
       }
    }
    __syncwarp();
@@ -133,12 +118,77 @@ __device__ __forceinline__ void countPlane(const T (&v)[32], WordCarry<KMAX> &c,
    }
 }
 
+// One warp counts work item `it` (31 x 31 cells, D planes) of field `a` into the CTA's histogram
+// and all-zeros / all-ones totals. INNER: the field is at least 32 x 32 in x and y with a positive
+// row stride below 2^32 / 31 bytes; edge tiles are then shifted back inside the field (their cells
+// already counted by the neighbouring tile are masked out), so no load needs clamping.
+template <typename T, int KMAX, int CLS0, int CLS1, bool INNER>
+__device__ __forceinline__ void wordItem(const WordTask &a, long long it, const T *tlo, const T *thi,
+                                         uint32_t (*sRow)[32], uint32_t *sHist, unsigned long long (*sEnds)[2])
+{
+   const int lane = threadIdx.x & 31;
+   const T *__restrict__ F = (const T *)a.f;
+   const uint32_t syb = (uint32_t)(a.sy * (int64_t)sizeof(T));
+   const int ix = (int)(it % a.nChunkX);
+   const long long rest = it / a.nChunkX;
+   const int iy = (int)(rest % a.nTileY);
+   const int iz = (int)(rest / a.nTileY);
+   // this item's cells: x in [xs, xe), y in [ys, ye), z in [z0, z0 + nPln)
+   const int xs = 31 * ix, ys = 31 * iy, z0 = kWdD * iz;
+   const int xe = min(xs + 31, a.X - 1), ye = min(ys + 31, a.Y - 1);
+   const int nPln = min(kWdD, a.Z - 1 - z0);
+   // tile origin: bit b of a word is x0 + b, lane l counts the row pair y0 + l
+   const int x0 = INNER ? min(xs, a.X - 32) : xs;
+   const int y0 = INNER ? min(ys, a.Y - 32) : ys;
+   const int nRow = INNER ? 32 : min(32, a.Y - y0);
+   const bool xin = INNER || x0 + lane < a.X;
+   const T *base = F + (long long)(INNER ? x0 + lane : min(x0 + lane, a.X - 1)) * a.sx + (long long)y0 * a.sy +
+                   (long long)z0 * a.sz;
+   const uint32_t vm = (y0 + lane >= ys && y0 + lane < ye)
+                          ? ((0xFFFFFFFFu >> (32 - (xe - x0))) & (0xFFFFFFFFu << (xs - x0)))
+                          : 0u;
+   WordCarry<KMAX> c;
+#pragma unroll
+   for (int k = 0; k < KMAX; k++) { c.n0[k] = c.n1[k] = 0; c.pw[k] = c.pn[k] = 0; }
+   for (int p = 0; p <= nPln; ++p) {
+      T v[32];
+      loadPlane<T, INNER>(v, base + (long long)p * a.sz, a.sy, syb, nRow);
+      countPlane<T, KMAX, CLS0, CLS1>(v, c, a.m, tlo, thi, xin, lane, vm, p == 0, sRow, sHist);
+   }
+#pragma unroll
+   for (int k = 0; k < KMAX; k++) {
+      const unsigned long long s0 = __reduce_add_sync(FULL, c.n0[k]);
+      const unsigned long long s1 = __reduce_add_sync(FULL, c.n1[k]);
+      if (lane == 0) {
+         if (s0) { atomicAdd(&sEnds[k][0], s0); }
+         if (s1) { atomicAdd(&sEnds[k][1], s1); }
+      }
+   }
+}
+
+// Add a CTA's counts of one field to its output rows (whole CTA, after a barrier): mixed codes as
+// counted, 0 / 255 from the all-zeros / all-ones totals; with `complement` the map was counted
+// negated, so code c belongs in bin 255 - c. Clears the counts for the next field.
+template <int KMAX>
+__device__ void flushWords(const WordTask &a, uint32_t *sHist, unsigned long long (*sEnds)[2])
+{
+   for (int i = threadIdx.x; i < a.K * 256; i += blockDim.x) {
+      const int k = i >> 8, c = i & 255;
+      unsigned long long v = sHist[i];
+      if (c == 0) { v += sEnds[k][0]; }
+      if (c == 255) { v += sEnds[k][1]; }
+      const int cc = a.complement ? 255 - c : c;
+      if (v) { atomicAdd((unsigned long long *)(a.out + (size_t)a.outRow[k] * 256 + cc), v); }
+      sHist[i] = 0;
+   }
+   __syncthreads();
+   if (threadIdx.x < KMAX * 2) { (&sEnds[0][0])[threadIdx.x] = 0; }
+   __syncthreads();
+}
+
 // One launch counts K = KMAX thresholds of classes CLS0 (and CLS1), compile-time constants.
-// INNER: the field is at least 32 x 32 in x and y with a positive row stride below 2^32 / 31
-// bytes; edge tiles are then shifted back inside the field (their cells already counted by the
-// neighbouring tile are masked out), so no load needs clamping.
 template <typename T, int KMAX, int CLS0, int CLS1, bool INNER, int MINB>
-__global__ void __launch_bounds__(kWdWarps * 32, MINB) wordBPFD(const __grid_constant__ WordArgs a)
+__global__ void __launch_bounds__(kWdWarps * 32, MINB) wordBPFD(const __grid_constant__ WordTask a)
 {
    __shared__ uint32_t sHist[KMAX * 256];
    __shared__ unsigned long long sEnds[KMAX][2];  // all-zeros, all-ones cells
@@ -153,62 +203,19 @@ __global__ void __launch_bounds__(kWdWarps * 32, MINB) wordBPFD(const __grid_con
       tlo[k] = (T)a.tlo[k];
       thi[k] = (T)a.thi[k];
    }
-   const int lane = threadIdx.x & 31;
    const long long gw = (long long)blockIdx.x * kWdWarps + (threadIdx.x >> 5);
    const long long nw = (long long)gridDim.x * kWdWarps;
-   const T *__restrict__ F = (const T *)a.f;
-   const uint32_t syb = (uint32_t)(a.sy * (int64_t)sizeof(T));
    uint32_t (*sRow)[32] = sRows[threadIdx.x >> 5];
 
    for (long long it = gw; it < a.nItems; it += nw) {
-      const int ix = (int)(it % a.nChunkX);
-      const long long rest = it / a.nChunkX;
-      const int iy = (int)(rest % a.nTileY);
-      const int iz = (int)(rest / a.nTileY);
-      // this item's cells: x in [xs, xe), y in [ys, ye), z in [z0, z0 + nPln)
-      const int xs = 31 * ix, ys = 31 * iy, z0 = kWdD * iz;
-      const int xe = min(xs + 31, a.X - 1), ye = min(ys + 31, a.Y - 1);
-      const int nPln = min(kWdD, a.Z - 1 - z0);
-      // tile origin: bit b of a word is x0 + b, lane l counts the row pair y0 + l
-      const int x0 = INNER ? min(xs, a.X - 32) : xs;
-      const int y0 = INNER ? min(ys, a.Y - 32) : ys;
-      const int nRow = INNER ? 32 : min(32, a.Y - y0);
-      const bool xin = INNER || x0 + lane < a.X;
-      const T *base = F + (long long)(INNER ? x0 + lane : min(x0 + lane, a.X - 1)) * a.sx + (long long)y0 * a.sy +
-                      (long long)z0 * a.sz;
-      const uint32_t vm = (y0 + lane >= ys && y0 + lane < ye)
-                             ? ((0xFFFFFFFFu >> (32 - (xe - x0))) & (0xFFFFFFFFu << (xs - x0)))
-                             : 0u;
-      WordCarry<KMAX> c;
-#pragma unroll
-      for (int k = 0; k < KMAX; k++) { c.n0[k] = c.n1[k] = 0; c.pw[k] = c.pn[k] = 0; }
-      for (int p = 0; p <= nPln; ++p) {
-         T v[32];
-         loadPlane<T, INNER>(v, base + (long long)p * a.sz, a.sy, syb, nRow);
-         countPlane<T, KMAX, CLS0, CLS1>(v, c, a, tlo, thi, xin, lane, vm, p == 0, sRow, sHist);
-      }
-#pragma unroll
-      for (int k = 0; k < KMAX; k++) {
-         const unsigned long long s0 = __reduce_add_sync(FULL, c.n0[k]);
-         const unsigned long long s1 = __reduce_add_sync(FULL, c.n1[k]);
-         if (lane == 0) {
-            if (s0) { atomicAdd(&sEnds[k][0], s0); }
-            if (s1) { atomicAdd(&sEnds[k][1], s1); }
-         }
-      }
+      wordItem<T, KMAX, CLS0, CLS1, INNER>(a, it, tlo, thi, sRow, sHist, sEnds);
    }
    __syncthreads();
-   for (int i = threadIdx.x; i < KMAX * 256; i += blockDim.x) {
-      const int k = i >> 8, c = i & 255;
-      unsigned long long v = sHist[i];
-      if (c == 0) { v += sEnds[k][0]; }
-      if (c == 255) { v += sEnds[k][1]; }
-      if (v) { atomicAdd((unsigned long long *)(a.out + (size_t)a.outRow[k] * 256 + c), v); }
-   }
+   flushWords<KMAX>(a, sHist, sEnds);
 }
 
 template <typename T, int KMAX, int CLS0, int CLS1, bool INNER>
-static int launchWordsI(const WordArgs &a, cudaStream_t s)
+static int launchWordsI(const WordTask &a, cudaStream_t s)
 {
    static int blocksPerSM = -1;
    auto kern = wordBPFD<T, KMAX, CLS0, CLS1, INNER, (INNER && sizeof(T) == 4) ? WORDS_MINB_F32 : 2>;
@@ -226,7 +233,7 @@ static int launchWordsI(const WordArgs &a, cudaStream_t s)
 }
 
 template <typename T, int KMAX, int CLS0, int CLS1>
-static int launchWordsT(const WordArgs &a, cudaStream_t s)
+static int launchWordsT(const WordTask &a, cudaStream_t s)
 {
    const int64_t syb = a.sy * (int64_t)sizeof(T);
    const bool inner = a.X >= 32 && a.Y >= 32 && syb > 0 && syb * 31 < (int64_t)1 << 32;
@@ -234,7 +241,7 @@ static int launchWordsT(const WordArgs &a, cudaStream_t s)
 }
 
 template <typename T>
-static int dispatchWords(const WordArgs &a, cudaStream_t s)
+static int dispatchWords(const WordTask &a, cudaStream_t s)
 {
    if (a.K == 2) {
       if (a.cls[0] == a.cls[1]) {
@@ -262,7 +269,7 @@ static int dispatchWords(const WordArgs &a, cudaStream_t s)
 int launchWords(const FusedArgs &f, int enc, const uint32_t *masks, cudaStream_t s)
 {
    if (f.K < 1 || f.K > 2) { return MKF_ERR_UNSUPPORTED; }
-   WordArgs a;
+   WordTask a;
    memset(&a, 0, sizeof(a));
    a.f = f.f;
    a.sx = f.sx; a.sy = f.sy; a.sz = f.sz;
@@ -283,6 +290,114 @@ int launchWords(const FusedArgs &f, int enc, const uint32_t *masks, cudaStream_t
    a.nItems = (long long)a.nChunkX * a.nTileY * a.nSlabZ;
    if (enc == ENC_F32) { return dispatchWords<float>(a, s); }
    return dispatchWords<double>(a, s);
+}
+
+// ---------------------------------------------------------------- many fields, one launch
+
+// Batched instantiations (WordTask::variant): 0 one threshold ">", 1 one threshold ">=" (a "<" or
+// "<=" threshold is counted as the complement of ">=" or ">"), 2 one threshold of another relation,
+// 3 two thresholds; + 4 for fields whose edge items can be shifted inside (INNER).
+
+// A CTA takes chunks of consecutive work items from a global counter; chunks never span fields.
+// When the next chunk belongs to another field, the CTA adds its counts of the previous field to
+// that field's output rows first. One kernel per element type, so that each keeps its register
+// budget (FP32 tiles need more warps in flight per byte).
+template <typename T, int MINB>
+__global__ void __launch_bounds__(kWdWarps * 32, MINB) wordBatch(const __grid_constant__ WordBatchArgs b)
+{
+   __shared__ uint32_t sHist[2 * 256];
+   __shared__ unsigned long long sEnds[2][2];
+   __shared__ uint32_t sRows[kWdWarps][2][32];
+   __shared__ WordTask F;
+   __shared__ int sChunk;
+   for (int i = threadIdx.x; i < 2 * 256; i += blockDim.x) { sHist[i] = 0; }
+   if (threadIdx.x < 4) { (&sEnds[0][0])[threadIdx.x] = 0; }
+   const int warp = threadIdx.x >> 5;
+   uint32_t (*sRow)[32] = sRows[warp];
+   int cur = -1;
+   for (;;) {
+      if (threadIdx.x == 0) { sChunk = (int)atomicAdd(b.counter, 1u); }
+      __syncthreads();
+      const int c = sChunk;
+      __syncthreads();
+      if (c >= b.nChunks) { break; }
+      const BatchChunk ch = b.chunks[c];
+      if (ch.field != cur) {
+         if (cur >= 0) { flushWords<2>(F, sHist, sEnds); }
+         const uint32_t *src = reinterpret_cast<const uint32_t *>(b.tasks + ch.field);
+         for (int i = threadIdx.x; i < (int)(sizeof(WordTask) / 4); i += blockDim.x) {
+            reinterpret_cast<uint32_t *>(&F)[i] = src[i];
+         }
+         __syncthreads();
+         cur = ch.field;
+      }
+      T tlo[2], thi[2];
+      tlo[0] = (T)F.tlo[0]; thi[0] = (T)F.thi[0];
+      tlo[1] = (T)F.tlo[1]; thi[1] = (T)F.thi[1];
+      for (long long it = ch.begin + warp; it < ch.end; it += kWdWarps) {
+         switch (F.variant) {
+            case 0: wordItem<T, 1, kGT, kGT, false>(F, it, tlo, thi, sRow, sHist, sEnds); break;
+            case 1: wordItem<T, 1, kGE, kGE, false>(F, it, tlo, thi, sRow, sHist, sEnds); break;
+            case 2: wordItem<T, 1, kGEN, kGEN, false>(F, it, tlo, thi, sRow, sHist, sEnds); break;
+            case 3: wordItem<T, 2, kGEN, kGEN, false>(F, it, tlo, thi, sRow, sHist, sEnds); break;
+            case 4: wordItem<T, 1, kGT, kGT, true>(F, it, tlo, thi, sRow, sHist, sEnds); break;
+            case 5: wordItem<T, 1, kGE, kGE, true>(F, it, tlo, thi, sRow, sHist, sEnds); break;
+            case 6: wordItem<T, 1, kGEN, kGEN, true>(F, it, tlo, thi, sRow, sHist, sEnds); break;
+            default: wordItem<T, 2, kGEN, kGEN, true>(F, it, tlo, thi, sRow, sHist, sEnds); break;
+         }
+      }
+   }
+   if (cur >= 0) {
+      __syncthreads();
+      flushWords<2>(F, sHist, sEnds);
+   }
+}
+
+// Fill a word task from a field with one or two varying thresholds (sorted rows and bounds in
+// `f`, relation masks in `masks`): relation classes, the batched variant and the item grid.
+void prepareWordTask(WordTask &a, int enc)
+{
+   int kind;
+   for (int k = 0; k < a.K; k++) {
+      const uint32_t m = a.m[k] & BMC_AL;
+      a.cls[k] = (m == BMC_GT) ? kGT : (m == (BMC_GT | BMC_EQ)) ? kGE : (m == BMC_LT) ? kLT : (m == (BMC_LT | BMC_EQ)) ? kLE : kGEN;
+   }
+   a.complement = 0;
+   if (a.K == 2) {
+      kind = 3;
+   } else {
+      switch (a.cls[0]) {
+         case kGT: kind = 0; break;
+         case kGE: kind = 1; break;
+         case kLT: kind = 1; a.complement = 1; break;  // f < t  is  !(f >= t)
+         case kLE: kind = 0; a.complement = 1; break;  // f <= t is  !(f > t)
+         default: kind = 2; break;
+      }
+   }
+   const int64_t syb = a.sy * (enc == ENC_F32 ? 4 : 8);
+   const bool inner = a.X >= 32 && a.Y >= 32 && syb > 0 && syb * 31 < ((int64_t)1 << 32);
+   a.variant = kind + (inner ? 4 : 0);
+   a.nChunkX = (a.X - 1 + 30) / 31;
+   a.nTileY = (a.Y - 1 + 30) / 31;
+   a.nSlabZ = (a.Z - 1 + kWdD - 1) / kWdD;
+   a.nItems = (long long)a.nChunkX * a.nTileY * a.nSlabZ;
+}
+
+int launchWordsBatch(const WordBatchArgs &b, int enc, cudaStream_t s)
+{
+   static int blocksPerSM[2] = {-1, -1};
+   const int e = enc == ENC_F32 ? 0 : 1;
+   auto kern = e == 0 ? wordBatch<float, 3> : wordBatch<double, 2>;
+   if (blocksPerSM[e] < 0) {
+      int n = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, kWdWarps * 32, 0);
+      blocksPerSM[e] = n > 0 ? n : 1;
+   }
+   long long grid = (long long)smCount() * blocksPerSM[e];
+   if (grid > b.nChunks) { grid = b.nChunks; }
+   if (grid < 1) { grid = 1; }
+   kern<<<(unsigned)grid, kWdWarps * 32, 0, s>>>(b);
+   return cudaFail(cudaGetLastError(), "wordBatch launch");
 }
 
 }  // namespace mkf
