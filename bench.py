@@ -323,8 +323,11 @@ def reference_sample(f: np.ndarray, planes: int, threads: int):
 
 
 def calibrate_planes(f: np.ndarray, threads: int, target_s: float, max_planes: int) -> int:
-    dt, _, _, _ = reference_sample(f, 2, threads)
-    return int(max(2, min(max_planes, 2 * target_s / max(dt, 1e-4))))
+    """Plane pairs per sample for about target_s seconds of reference work (timed on 8 planes, so
+    that thread start-up is a small part of the measurement)."""
+    n = min(8, max_planes)
+    dt, _, _, _ = reference_sample(f, n, threads)
+    return int(max(2, min(max_planes, n * target_s / max(dt, 1e-4))))
 
 
 def cpu_baseline(f: np.ndarray, target_s: float = 10.0):
@@ -343,7 +346,7 @@ def run_reference(args, rank, world):
     threads = cpu_threads()
     max_planes = 128
     f = grf_numpy(max_planes + 1, N_SIDE, N_SIDE, SEED)  # a slab of the same kind of field (1 GB)
-    planes = calibrate_planes(f, threads, 1.0, max_planes)  # about 1 s of reference work per step
+    planes = calibrate_planes(f, threads, 0.5, max_planes)  # about 0.5 s of reference work per step
     for _ in range(args.warmup):
         reference_sample(f, planes, threads)
     times = []
