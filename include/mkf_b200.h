@@ -110,6 +110,57 @@ int mkfBatchPlanDestroy(MKFBatchPlan *plan);
 /* One-shot: create a plan, launch it on `stream`, wait for it and destroy it (synchronous). */
 int mkfBatchBPFD(uint64_t *pBPFD, const MKFFieldDesc *pF, const MKFThreshSet *pT, int nF, int flags, void *stream);
 
+/* ---- serving: a request loop for in-situ analysis (no original counterpart) ----
+ * Clients (any host threads) submit fields with their thresholds; a worker thread of the server
+ * admits requests in arrival order while a device-memory budget allows, copies host fields to
+ * the device on a copy stream, and packs every request admitted since the last launch into the
+ * next persistent batched launch, while the previous launch may still run (two launch streams).
+ * Counts stay in device memory (budget-accounted) until mkfServerRelease, or are copied to
+ * hostOut when the request names one. A device field must stay valid and unchanged until its
+ * request is done; a host field must be pinned (cudaMallocHost / cudaHostRegister) and planar. */
+typedef struct MKFServer MKFServer;
+typedef struct
+{
+   uint64_t hbmBudget;          /* device bytes for staged host fields + counts (0 = 64 GiB) */
+   int32_t maxFieldsPerLaunch;  /* 0 = 256 */
+   int32_t device;              /* CUDA device ordinal */
+} MKFServerConfig;
+
+#define MKF_REQ_HOST_FIELD 0x1  /* field.p is pinned host memory: the server stages it */
+
+typedef struct
+{
+   MKFFieldDesc field;
+   MKFThreshSet thresh;         /* copied at submission */
+   uint32_t flags;              /* MKF_REQ_* */
+   uint32_t pad_;
+   uint64_t *hostOut;           /* optional host uint64_t[nT][256]; then the device counts are freed */
+} MKFRequest;
+
+typedef struct
+{
+   uint64_t completed, failed, launches;  /* since creation or the last reset */
+   uint32_t maxFieldsInLaunch, pad_;
+   double meanFieldsInLaunch;
+   double p50, p99, mean, max;  /* latency in seconds, submission to completion seen by the server */
+   uint64_t deviceBytesInUse;   /* budget in use now (staged fields + held counts) */
+} MKFServerStats;
+
+int mkfServerCreate(MKFServer **pServer, const MKFServerConfig *cfg);
+/* Non-blocking and thread-safe; returns a ticket. */
+int mkfServerSubmit(MKFServer *server, const MKFRequest *req, uint64_t *ticket);
+/* Wait up to timeoutSec for a ticket: MKF_OK with *pDevCounts = its device counts (NULL when
+ * copied to hostOut) and its latency, MKF_ERR_TIMEOUT, or the request's own error (e.g.
+ * MKF_ERR_NOMEM for a request larger than the budget). */
+int mkfServerWait(MKFServer *server, uint64_t ticket, double timeoutSec, const uint64_t **pDevCounts, double *latencySec);
+/* Copy a finished ticket's device counts to dst (host or device), synchronously on `stream`. */
+int mkfServerCopyCounts(MKFServer *server, uint64_t ticket, uint64_t *dst, void *stream);
+/* Forget a finished ticket and free its device counts. */
+int mkfServerRelease(MKFServer *server, uint64_t ticket);
+int mkfServerStats(MKFServer *server, MKFServerStats *stats, int reset);
+/* Finishes every submitted request, then frees the server (tickets become invalid). */
+int mkfServerDestroy(MKFServer *server);
+
 /* ---- measures (closest original: mkfSelectMeasuresBPFD, mkfUtil.c:94) ---- */
 /* For each of nSets distributions (host uint64_t[nSets][256]) write, in double:
  *   r[4*i+0] V   = number of cells whose corner 0 is set (volume in cell units)

@@ -15,11 +15,12 @@ import subprocess
 import numpy as np
 
 from . import _lib
-from ._lib import (BMC_AL, BMC_EQ, BMC_GT, BMC_LT, ENC_F32, ENC_F64, MKF_F_ACCUMULATE, BinMapF64, BMFieldInfo,
-                   BMOrg, ConstFieldPtr, KernInfo, MKFError, MKFFieldDesc, MKFThreshSet, check, lib)
+from ._lib import (BMC_AL, BMC_EQ, BMC_GT, BMC_LT, ENC_F32, ENC_F64, MKF_F_ACCUMULATE, MKF_REQ_HOST_FIELD, BinMapF64,
+                   BMFieldInfo, BMOrg, ConstFieldPtr, KernInfo, MKFError, MKFFieldDesc, MKFRequest, MKFServerConfig,
+                   MKFServerStats, MKFThreshSet, check, lib)
 
 __all__ = [
-    "build", "lib", "MKFError", "BatchPlan", "relation_mask", "field_bpfd", "field_bpfd_host", "batch_bpfd",
+    "build", "lib", "MKFError", "BatchPlan", "Server", "relation_mask", "field_bpfd", "field_bpfd_host", "batch_bpfd",
     "bin_map_cuda", "get_bpfd", "get_bpfd_host", "measures", "measures_dev", "select_measures",
     "ENC_F32", "ENC_F64", "BMC_LT", "BMC_EQ", "BMC_GT", "BMC_AL",
 ]
@@ -186,6 +187,87 @@ class BatchPlan:
             _torch().cuda.synchronize()
             lib().mkfBatchPlanDestroy(self._h)
             self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """The request loop (mkfServerCreate): submit() fields as CUDA tensors (device-resident) or
+    pinned host tensors / arrays (staged by the server), wait() for their counts. Requests submitted
+    while others run are admitted into the next launch as the device-memory budget allows."""
+
+    def __init__(self, hbm_budget: int = 0, max_fields_per_launch: int = 0, device: int = 0):
+        cfg = MKFServerConfig(hbm_budget, max_fields_per_launch, device)
+        h = C.c_void_p()
+        check(lib().mkfServerCreate(C.byref(h), C.byref(cfg)), "mkfServerCreate")
+        self._h = h
+        self._keep = {}  # ticket -> objects the request points to
+
+    def submit(self, field, thresholds, mask=BMC_GT, host_out: bool = False) -> int:
+        """Queue one field (CUDA tensor, or a pinned CPU tensor / numpy array viewing pinned memory).
+        With host_out the counts come back as a numpy array from wait(); otherwise they stay on the
+        device until release()."""
+        th = _Thresholds(thresholds, mask)
+        req = MKFRequest()
+        if isinstance(field, np.ndarray):
+            enc = ENC_F32 if field.dtype == np.float32 else ENC_F64 if field.dtype == np.float64 else None
+            if enc is None or not field.flags["C_CONTIGUOUS"]:
+                raise TypeError("host fields must be C-contiguous float32/float64")
+            req.field = _field_desc(field.ctypes.data, enc, field.shape)
+            req.flags = MKF_REQ_HOST_FIELD
+        elif field.device.type == "cpu":
+            if not field.is_contiguous():
+                raise ValueError("host fields must be contiguous")
+            req.field = _field_desc(field.data_ptr(), _enc_of(field), field.shape)
+            req.flags = MKF_REQ_HOST_FIELD
+        else:
+            strides = None if field.is_contiguous() else field.stride()
+            req.field = _field_desc(field.data_ptr(), _enc_of(field), field.shape, strides)
+        req.thresh = th.ts
+        out = np.zeros((th.n, 256), np.uint64) if host_out else None
+        req.hostOut = out.ctypes.data if host_out else None
+        tk = C.c_uint64()
+        check(lib().mkfServerSubmit(self._h, C.byref(req), C.byref(tk)), "mkfServerSubmit")
+        self._keep[tk.value] = (field, out, th.n)
+        return tk.value
+
+    def wait(self, ticket: int, timeout: float = 60.0):
+        """Block until the ticket is done. Returns (counts, latency_s): a numpy (K, 256) uint64 array
+        for host_out requests (the ticket is then released), else the device address of the counts."""
+        dev = C.c_void_p()
+        lat = C.c_double()
+        check(lib().mkfServerWait(self._h, ticket, timeout, C.byref(dev), C.byref(lat)), "mkfServerWait")
+        field, out, n = self._keep[ticket]
+        if out is not None:
+            self.release(ticket)
+            return out, lat.value
+        return dev.value, lat.value
+
+    def counts(self, ticket: int) -> np.ndarray:
+        """Host copy of a finished ticket's device-resident counts."""
+        n = self._keep[ticket][2]
+        out = np.zeros((n, 256), np.uint64)
+        check(lib().mkfServerCopyCounts(self._h, ticket, out.ctypes.data, None), "mkfServerCopyCounts")
+        return out
+
+    def release(self, ticket: int) -> None:
+        check(lib().mkfServerRelease(self._h, ticket), "mkfServerRelease")
+        self._keep.pop(ticket, None)
+
+    def stats(self, reset: bool = False) -> dict:
+        st = MKFServerStats()
+        check(lib().mkfServerStats(self._h, C.byref(st), int(reset)), "mkfServerStats")
+        return {f: getattr(st, f) for f, _ in MKFServerStats._fields_ if f != "pad_"}
+
+    def close(self):
+        if self._h:
+            lib().mkfServerDestroy(self._h)
+            self._h = None
+            self._keep.clear()
 
     def __del__(self):
         try:

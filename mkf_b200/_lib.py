@@ -70,6 +70,25 @@ class MKFThreshSet(C.Structure):
 
 # (name, restype, argtypes) of every exported C entry point
 _P = C.c_void_p
+MKF_REQ_HOST_FIELD = 0x1
+
+
+class MKFServerConfig(C.Structure):
+    _fields_ = [("hbmBudget", C.c_uint64), ("maxFieldsPerLaunch", C.c_int32), ("device", C.c_int32)]
+
+
+class MKFRequest(C.Structure):
+    _fields_ = [("field", MKFFieldDesc), ("thresh", MKFThreshSet), ("flags", C.c_uint32), ("pad_", C.c_uint32),
+                ("hostOut", C.c_void_p)]
+
+
+class MKFServerStats(C.Structure):
+    _fields_ = [("completed", C.c_uint64), ("failed", C.c_uint64), ("launches", C.c_uint64),
+                ("maxFieldsInLaunch", C.c_uint32), ("pad_", C.c_uint32), ("meanFieldsInLaunch", C.c_double),
+                ("p50", C.c_double), ("p99", C.c_double), ("mean", C.c_double), ("max", C.c_double),
+                ("deviceBytesInUse", C.c_uint64)]
+
+
 _SIG = [
     ("binMapCUDA", _P, [C.POINTER(KernInfo), _P, C.POINTER(BMOrg), C.POINTER(BMFieldInfo), C.POINTER(BinMapF64)]),
     ("binMapCUDACleanup", None, []),
@@ -109,6 +128,13 @@ _SIG = [
     ("mkfBatchPlanLaunchGraph", C.c_int, [_P, _P]),
     ("mkfBatchPlanDestroy", C.c_int, [_P]),
     ("mkfBatchBPFD", C.c_int, [_P, C.POINTER(MKFFieldDesc), C.POINTER(MKFThreshSet), C.c_int, C.c_int, _P]),
+    ("mkfServerCreate", C.c_int, [C.POINTER(C.c_void_p), C.POINTER(MKFServerConfig)]),
+    ("mkfServerSubmit", C.c_int, [_P, C.POINTER(MKFRequest), C.POINTER(C.c_uint64)]),
+    ("mkfServerWait", C.c_int, [_P, C.c_uint64, C.c_double, C.POINTER(C.c_void_p), C.POINTER(C.c_double)]),
+    ("mkfServerCopyCounts", C.c_int, [_P, C.c_uint64, _P, _P]),
+    ("mkfServerRelease", C.c_int, [_P, C.c_uint64]),
+    ("mkfServerStats", C.c_int, [_P, C.POINTER(MKFServerStats), C.c_int]),
+    ("mkfServerDestroy", C.c_int, [_P]),
     ("mkfMeasuresF64", C.c_int, [_P, _P, C.c_int]),
     ("mkfMeasuresF64Dev", C.c_int, [_P, _P, C.c_int, _P]),
 ]

@@ -6,7 +6,6 @@
 #include "fused.cuh"
 
 namespace mkf {
-int fieldBPFD(uint64_t *out, const MKFFieldDesc *pF, const MKFThreshSet *pT, int flags, cudaStream_t s, const int *rowBase);
 void measures(double r[4], const uint64_t h[256]);
 extern const uint8_t kGroupOf[256];
 extern const int kWK[22];

@@ -86,6 +86,10 @@ struct WordBatchArgs
 };
 
 struct ConstEntry { int row, bin; };
+// Count one field for any thresholds (fused.cu): constant maps, one pass per relation class.
+// rowBase[i] is the output row of threshold i (NULL = identity).
+int fieldBPFD(uint64_t *out, const MKFFieldDesc *pF, const MKFThreshSet *pT, int flags, cudaStream_t s, const int *rowBase);
+
 enum { kPlanSingle = 0, kPlanThermo = 1, kPlanWords = 2 };
 int planBatchField(const MKFFieldDesc *pF, const MKFThreshSet *pT, int rowBase, FieldTask &t, WordTask &w,
                    std::vector<ConstEntry> &consts, bool &anyVarying);
