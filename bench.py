@@ -99,11 +99,33 @@ def grf_numpy(nz, ny, nx, seed):
     return np.ascontiguousarray(f.ravel())
 
 
+def ball_field(shape_zyx, rng, g, device, dtype):
+    """Max over 1-64 balls (centres uniform in the box, radii uniform in [2, 40]) of r - |x - c|,
+    plus N(0, 0.1) noise. The max is formed inside each ball's bounding box only: elsewhere the
+    value stays far below zero, which maps the same at thresholds near 0."""
+    import torch
+
+    Z, Y, X = shape_zyx
+    f = torch.full((Z, Y, X), -50.0, dtype=dtype, device=device)
+    for _b in range(int(rng.integers(1, 65))):
+        c = rng.random(3) * np.array([X, Y, Z])
+        r = float(rng.uniform(2, 40))
+        lo3 = [max(0, int(np.floor(c[i] - r - 1))) for i in range(3)]
+        hi3 = [min((X, Y, Z)[i], int(np.ceil(c[i] + r + 2))) for i in range(3)]
+        if min(hi3[i] - lo3[i] for i in range(3)) <= 0:
+            continue
+        zz = torch.arange(lo3[2], hi3[2], device=device, dtype=dtype).view(-1, 1, 1) - c[2]
+        yy = torch.arange(lo3[1], hi3[1], device=device, dtype=dtype).view(1, -1, 1) - c[1]
+        xx = torch.arange(lo3[0], hi3[0], device=device, dtype=dtype).view(1, 1, -1) - c[0]
+        v = r - torch.sqrt(zz * zz + yy * yy + xx * xx)
+        box = f[lo3[2]:hi3[2], lo3[1]:hi3[1], lo3[0]:hi3[0]]
+        torch.maximum(box, v, out=box)
+    f.add_(torch.randn((Z, Y, X), dtype=dtype, device=device, generator=g).mul_(0.1))
+    return f
+
+
 def ball_fields(n_fields, seed, device, lo=17, hi=400, dtype=None):
-    """The uneven batch: each axis uniform in [lo, hi]; content = max over 1-64 balls (centres
-    uniform in the box, radii uniform in [2, 40]) of r - |x - c|, plus N(0, 0.1) noise. The max
-    is formed inside each ball's bounding box only: elsewhere the value stays far below zero,
-    which maps the same at threshold 0."""
+    """The uneven batch: each axis uniform in [lo, hi], ball content (ball_field)."""
     import torch
 
     dtype = dtype or torch.float32
@@ -112,22 +134,7 @@ def ball_fields(n_fields, seed, device, lo=17, hi=400, dtype=None):
     fields = []
     for _ in range(n_fields):
         X, Y, Z = (int(v) for v in rng.integers(lo, hi + 1, size=3))
-        f = torch.full((Z, Y, X), -50.0, dtype=dtype, device=device)
-        for _b in range(int(rng.integers(1, 65))):
-            c = rng.random(3) * np.array([X, Y, Z])
-            r = float(rng.uniform(2, 40))
-            lo3 = [max(0, int(np.floor(c[i] - r - 1))) for i in range(3)]
-            hi3 = [min((X, Y, Z)[i], int(np.ceil(c[i] + r + 2))) for i in range(3)]
-            if min(hi3[i] - lo3[i] for i in range(3)) <= 0:
-                continue
-            zz = torch.arange(lo3[2], hi3[2], device=device, dtype=dtype).view(-1, 1, 1) - c[2]
-            yy = torch.arange(lo3[1], hi3[1], device=device, dtype=dtype).view(1, -1, 1) - c[1]
-            xx = torch.arange(lo3[0], hi3[0], device=device, dtype=dtype).view(1, 1, -1) - c[0]
-            v = r - torch.sqrt(zz * zz + yy * yy + xx * xx)
-            box = f[lo3[2]:hi3[2], lo3[1]:hi3[1], lo3[0]:hi3[0]]
-            torch.maximum(box, v, out=box)
-        f.add_(torch.randn((Z, Y, X), dtype=dtype, device=device, generator=g).mul_(0.1))
-        fields.append(f)
+        fields.append(ball_field((Z, Y, X), rng, g, device, dtype))
     torch.cuda.synchronize(device)
     return fields
 
@@ -193,6 +200,122 @@ def run_batch_workload(dev, n_fields=512, seed=SEED + 3, reps=3):
     del fields, outs
     torch.cuda.empty_cache()
     return res
+
+
+def serving_pool(dev, n=48, seed=SEED + 4):
+    """Fields a serving run draws from: voxel counts log-uniform in [32^3, 512^3], aspect ratios up
+    to 4:1, 70 % FP32 / 30 % FP64, ball content; even entries stay on the device, odd ones are
+    pinned host copies (the server stages those)."""
+    import torch
+
+    rng = np.random.default_rng(seed)
+    g = torch.Generator(device=dev).manual_seed(seed)
+    pool = []
+    for i in range(n):
+        vox = float(np.exp(rng.uniform(np.log(32.0 ** 3), np.log(512.0 ** 3))))
+        a = np.exp(rng.uniform(-np.log(2.0), np.log(2.0), size=3))  # max / min <= 4
+        a = a / np.cbrt(a.prod())
+        X, Y, Z = (max(2, int(round(np.cbrt(vox) * v))) for v in a)
+        dt = torch.float32 if rng.random() < 0.7 else torch.float64
+        f = ball_field((Z, Y, X), rng, g, dev, dt)
+        if i % 2:
+            h = torch.empty(f.shape, dtype=dt, pin_memory=True)
+            h.copy_(f)
+            del f
+            f = h
+        pool.append(f)
+    torch.cuda.synchronize(dev)
+    return pool
+
+
+def run_serving_workload(dev, rates=(100, 500, 1000, 2000, 5000), max_requests=10000, seconds=3.0,
+                         seed=SEED + 5):
+    """Poisson request streams at each rate (min(10000, rate x 3 s) requests, so every rate runs a
+    few seconds): each request takes a random pool field and 1-8 thresholds in [-2, 2] (relation
+    >), counts stay on the device until the client has waited for them and released them. Reports
+    p50/p99 latency (submission to completion) and throughput per rate, the saturated throughput
+    (every request submitted at once), and the plain per-field drop-in call on the same mix."""
+    import threading
+
+    import torch
+
+    import mkf_b200
+
+    pool = serving_pool(dev)
+    rng = np.random.default_rng(seed)
+    srv = mkf_b200.Server(hbm_budget=64 << 30)
+
+    def requests(n):
+        idx = rng.integers(0, len(pool), size=n)
+        ks = rng.integers(1, 9, size=n)
+        return [(int(i), np.sort(rng.uniform(-2, 2, size=int(k)))) for i, k in zip(idx, ks)]
+
+    def stream(reqs, rate):
+        gaps = rng.exponential(1.0 / rate, size=len(reqs)) if rate else np.zeros(len(reqs))
+        tickets = [None] * len(reqs)
+        done = threading.Event()
+
+        def waiter():
+            for j in range(len(reqs)):
+                while tickets[j] is None:
+                    time.sleep(0.0001)
+                srv.wait(tickets[j], timeout=600)
+                srv.release(tickets[j])
+            done.set()
+
+        w = threading.Thread(target=waiter)
+        w.start()
+        t0 = time.perf_counter()
+        due = t0
+        for j, (i, t) in enumerate(reqs):
+            due += gaps[j]
+            while True:
+                now = time.perf_counter()
+                if now >= due:
+                    break
+                if due - now > 0.0003:
+                    time.sleep(due - now - 0.0002)
+            tickets[j] = srv.submit(pool[i], t, mkf_b200.BMC_GT)
+        done.wait()
+        t1 = time.perf_counter()
+        w.join()
+        st = srv.stats(reset=True)
+        vox = sum(pool[i].numel() for i, _ in reqs)
+        h2d = sum(pool[i].numel() * pool[i].element_size() for i, _ in reqs if not pool[i].is_cuda)
+        return {"requests": len(reqs), "offered_per_s": rate, "fields_per_s": len(reqs) / (t1 - t0),
+                "gvoxel_per_s": vox / (t1 - t0) * 1e-9, "h2d_gb_per_s": h2d / (t1 - t0) * 1e-9,
+                "p50_ms": st["p50"] * 1e3, "p99_ms": st["p99"] * 1e3,
+                "launches": st["launches"], "mean_fields_per_launch": st["meanFieldsInLaunch"]}
+
+    stream(requests(200), 0)  # warm-up
+    per_rate = [stream(requests(int(min(max_requests, r * seconds))), r) for r in rates]
+    burst = stream(requests(2000), 0)
+
+    # the plain per-field call on a sample of the same mix: host fields copied first, then one
+    # binMapCUDA + mkfCUDAGetBPFDH per threshold, as a caller of the original library would
+    sample = requests(100)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for i, t in sample:
+        f = pool[i] if pool[i].is_cuda else pool[i].to(dev, non_blocking=True)
+        for tv in t:
+            pbm, org, _ = mkf_b200.bin_map_cuda(f, ">", float(tv))
+            mkf_b200.get_bpfd_host(pbm, org)
+    plain = len(sample) / (time.perf_counter() - t0)
+    srv.close()
+    del pool
+    torch.cuda.empty_cache()
+    return {
+        "workload": "Poisson requests, voxels log-uniform 32^3..512^3, aspect <= 4:1, 70% FP32, 1-8 thresholds, "
+                    "half device / half pinned host, 64 GB budget",
+        "per_rate": per_rate,
+        "saturated_fields_per_s": burst["fields_per_s"],
+        "saturated_h2d_gb_per_s": burst["h2d_gb_per_s"],
+        "bound": "host-to-device copies of the pinned-host half of the requests (PCIe) at saturation",
+        "saturated_p99_ms": burst["p99_ms"],
+        "plain_dropin_fields_per_s": plain,
+        "saturated_vs_plain": burst["fields_per_s"] / plain,
+    }
 
 
 # ---------------------------------------------------------------- clocks
@@ -483,6 +606,7 @@ def run_mkf(args, rank, world, local_rank):
     if world == 1 and not args.no_secondary:
         del fh, fh_np
         line["batched"] = run_batch_workload(dev)
+        line["serving"] = run_serving_workload(dev)
     print(json.dumps(line), flush=True)
 
 
