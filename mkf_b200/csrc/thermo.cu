@@ -144,14 +144,24 @@ struct ThermoShared
 #define THERMO_HROW 257
 #endif
 static constexpr int kHistRow = THERMO_HROW;
-__host__ __device__ constexpr size_t thermoDynBytes(int K) { return ((size_t)K * kHistRow + 32) * sizeof(uint32_t); }
+// Copies of the histogram, picked by lane: neighbouring cells (neighbouring lanes) often add to the
+// same (threshold, code) word in the same instruction, and each copy takes a share of those
+// same-address updates; the copies sit an odd multiple of 16 banks apart for K odd, 16 for K even.
+#ifndef THERMO_HCOPIES
+#define THERMO_HCOPIES 2
+#endif
+static constexpr int kHistCopies = THERMO_HCOPIES;
+__host__ __device__ constexpr size_t thermoDynBytes(int K)
+{
+   return ((size_t)K * kHistRow * kHistCopies + 32) * sizeof(uint32_t);
+}
 
 // Load one field's thresholds, build its rank table and clear the histogram (whole CTA).
 template <typename P>
 __device__ void ctaSetup(const P &a, ThermoShared &S, uint32_t *hist)
 {
    const int K = a.K;
-   for (int i = threadIdx.x; i < K * kHistRow; i += blockDim.x) { hist[i] = 0; }
+   for (int i = threadIdx.x; i < K * kHistRow * kHistCopies; i += blockDim.x) { hist[i] = 0; }
    for (int i = threadIdx.x; i < 64; i += blockDim.x) {
       S.tlo[i] = a.tlo[i];
       S.thi[i] = a.thi[i];
@@ -180,7 +190,10 @@ __device__ void ctaFlush(const P &a, ThermoShared &S, const uint32_t *hist)
    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
    for (int k = warp; k < K; k += kThWarps) {
       uint32_t s = 0;
-      for (int c = 1 + lane; c < 255; c += 32) { s += hist[k * kHistRow + c]; }
+      for (int c = 1 + lane; c < 255; c += 32) {
+#pragma unroll
+         for (int q = 0; q < kHistCopies; ++q) { s += hist[(q * K + k) * kHistRow + c]; }
+      }
       s = __reduce_add_sync(FULL, s);
       if (lane == 0) {
          const unsigned long long n1 = S.ones[k];
@@ -193,7 +206,9 @@ __device__ void ctaFlush(const P &a, ThermoShared &S, const uint32_t *hist)
    }
    for (int i = threadIdx.x; i < K * 256; i += blockDim.x) {
       const int c = i & 255;
-      const uint32_t v = hist[(i >> 8) * kHistRow + c];
+      uint32_t v = 0;
+#pragma unroll
+      for (int q = 0; q < kHistCopies; ++q) { v += hist[(q * K + (i >> 8)) * kHistRow + c]; }
       if (v && c != 0 && c != 255) {
          const int cc = a.complement ? 255 - c : c;
          atomicAdd((unsigned long long *)(a.out + (size_t)a.outRow[i >> 8] * 256 + cc), (unsigned long long)v);
@@ -235,8 +250,9 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
    const int lane = threadIdx.x & 31;
    const int K = a.K;
    const uint32_t nanRank = a.nanRank;
-   const uint32_t hist32 = (uint32_t)__cvta_generic_to_shared(sHist);
-   const uint32_t trash = hist32 + (uint32_t)(K * kHistRow + lane) * 4u;
+   const uint32_t histBase = (uint32_t)__cvta_generic_to_shared(sHist);
+   const uint32_t hist32 = histBase + (uint32_t)((lane & (kHistCopies - 1)) * K * kHistRow) * 4u;  // this lane's copy
+   const uint32_t trash = histBase + (uint32_t)(K * kHistRow * kHistCopies + lane) * 4u;
 
    const int ix = (int)(it % a.nSegX);
    const long long rest = it / a.nSegX;
@@ -472,13 +488,18 @@ static uint32_t thresholdKey(double t, int enc, bool ge)
 template <typename T, int TY, bool GE, int NSLOT, bool INNER>
 static int launchThermoT(const FusedArgs &a, cudaStream_t s)
 {
-   static int blocksPerSM = -1;
+   static int blocksPerSMofK[MKF_MAX_THRESH + 1] = {0};
+   static bool attr = false;
    auto kern = thermoBPFD<T, TY, GE, NSLOT, INNER>;
-   if (blocksPerSM < 0) {
-      // static + dynamic shared memory exceeds the default 48 KB for K > 23
+   if (!attr) {
+      // static + dynamic shared memory exceeds the default 48 KB for large K
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)thermoDynBytes(MKF_MAX_THRESH));
+      attr = true;
+   }
+   int &blocksPerSM = blocksPerSMofK[a.K];  // resident CTAs for this K's histogram size
+   if (blocksPerSM <= 0) {
       int n = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, kThWarps * 32, thermoDynBytes(MKF_MAX_THRESH));
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, kThWarps * 32, thermoDynBytes(a.K));
       blocksPerSM = n > 0 ? n : 1;
    }
    long long grid = (a.nItems + kThWarps - 1) / kThWarps;
