@@ -88,13 +88,14 @@ struct MKFBatchPlan
 {
    uint64_t *out = nullptr;
    size_t rows = 0;
-   FieldTask *dTasks = nullptr;     // thermometer-kernel fields
-   BatchChunk *dChunks = nullptr;
-   int nChunks = 0;
+   FieldTask *dTasks[2] = {nullptr, nullptr};  // thermometer-kernel fields, FP32 and FP64
+   BatchChunk *dChunks[2] = {nullptr, nullptr};
+   int nChunks[2] = {0, 0};
+   int maxK[2] = {0, 0};
    WordTask *dWTasks[2] = {nullptr, nullptr};  // word-kernel fields, FP32 and FP64
    BatchChunk *dWChunks[2] = {nullptr, nullptr};
    int nWChunks[2] = {0, 0};
-   unsigned *dCounter = nullptr;    // chunk counters: thermometer, words FP32, words FP64
+   unsigned *dCounter = nullptr;    // chunk counters: words FP32, words FP64, thermometer FP32, FP64
    std::vector<ConstEntry> consts;
    std::vector<unsigned long long> constCells;
    struct Fallback
@@ -118,9 +119,9 @@ static void freePlan(MKFBatchPlan *p)
    if (!p) { return; }
    if (p->graphExec) { cudaGraphExecDestroy(p->graphExec); }
    if (p->graph) { cudaGraphDestroy(p->graph); }
-   if (p->dTasks) { cudaFree(p->dTasks); }
-   if (p->dChunks) { cudaFree(p->dChunks); }
    for (int e = 0; e < 2; e++) {
+      if (p->dTasks[e]) { cudaFree(p->dTasks[e]); }
+      if (p->dChunks[e]) { cudaFree(p->dChunks[e]); }
       if (p->dWTasks[e]) { cudaFree(p->dWTasks[e]); }
       if (p->dWChunks[e]) { cudaFree(p->dWChunks[e]); }
    }
@@ -134,8 +135,8 @@ MKF_API int mkfBatchPlanCreate(MKFBatchPlan **pp, uint64_t *pBPFD, const MKFFiel
    *pp = nullptr;
    MKFBatchPlan *p = new MKFBatchPlan();
    p->out = pBPFD;
-   std::vector<FieldTask> tasks;
-   std::vector<BatchChunk> chunks;
+   std::vector<FieldTask> tasks[2];
+   std::vector<BatchChunk> chunks[2];
    std::vector<WordTask> wtasks[2];
    std::vector<BatchChunk> wchunks[2];
    size_t row = 0;
@@ -164,12 +165,14 @@ MKF_API int mkfBatchPlanCreate(MKFBatchPlan **pp, uint64_t *pBPFD, const MKFFiel
          w.out = pBPFD;
          wtasks[e].push_back(w);
       } else if (cells > 0 && kind == kPlanThermo) {
-         const int f = (int)tasks.size();
+         const int e = d->enc == ENC_F32 ? 0 : 1;
+         const int f = (int)tasks[e].size();
          for (long long b = 0; b < t.nItems; b += kChunkItems) {
-            chunks.push_back({f, 0, b, std::min<long long>(b + kChunkItems, t.nItems)});
+            chunks[e].push_back({f, 0, b, std::min<long long>(b + kChunkItems, t.nItems)});
          }
          t.out = pBPFD;
-         tasks.push_back(t);
+         tasks[e].push_back(t);
+         p->maxK[e] = std::max(p->maxK[e], t.K);
       } else if (cells > 0 && varying) {
          MKFBatchPlan::Fallback fb;
          fb.d = *d;
@@ -186,13 +189,14 @@ MKF_API int mkfBatchPlanCreate(MKFBatchPlan **pp, uint64_t *pBPFD, const MKFFiel
       row += (size_t)ts->nT;
    }
    p->rows = row;
-   cudaError_t e = cudaMalloc(&p->dCounter, 3 * sizeof(unsigned));
-   if (e == cudaSuccess && !tasks.empty()) {
-      e = cudaMalloc(&p->dTasks, tasks.size() * sizeof(FieldTask));
-      if (e == cudaSuccess) { e = cudaMalloc(&p->dChunks, chunks.size() * sizeof(BatchChunk)); }
-      if (e == cudaSuccess) { e = cudaMemcpy(p->dTasks, tasks.data(), tasks.size() * sizeof(FieldTask), cudaMemcpyHostToDevice); }
-      if (e == cudaSuccess) { e = cudaMemcpy(p->dChunks, chunks.data(), chunks.size() * sizeof(BatchChunk), cudaMemcpyHostToDevice); }
-      p->nChunks = (int)chunks.size();
+   cudaError_t e = cudaMalloc(&p->dCounter, 4 * sizeof(unsigned));
+   for (int k = 0; k < 2 && e == cudaSuccess; k++) {
+      if (tasks[k].empty()) { continue; }
+      e = cudaMalloc(&p->dTasks[k], tasks[k].size() * sizeof(FieldTask));
+      if (e == cudaSuccess) { e = cudaMalloc(&p->dChunks[k], chunks[k].size() * sizeof(BatchChunk)); }
+      if (e == cudaSuccess) { e = cudaMemcpy(p->dTasks[k], tasks[k].data(), tasks[k].size() * sizeof(FieldTask), cudaMemcpyHostToDevice); }
+      if (e == cudaSuccess) { e = cudaMemcpy(p->dChunks[k], chunks[k].data(), chunks[k].size() * sizeof(BatchChunk), cudaMemcpyHostToDevice); }
+      p->nChunks[k] = (int)chunks[k].size();
    }
    for (int k = 0; k < 2 && e == cudaSuccess; k++) {
       if (wtasks[k].empty()) { continue; }
@@ -219,8 +223,8 @@ static int planLaunchOn(MKFBatchPlan *p, cudaStream_t s)
    for (size_t i = 0; i < p->consts.size() && rc == MKF_OK; i++) {
       rc = launchConstBin(p->out, p->consts[i].row, p->consts[i].bin, p->constCells[i], s);
    }
-   if (rc == MKF_OK && (p->nChunks > 0 || p->nWChunks[0] > 0 || p->nWChunks[1] > 0)) {
-      e = cudaMemsetAsync(p->dCounter, 0, 3 * sizeof(unsigned), s);
+   if (rc == MKF_OK && (p->nChunks[0] > 0 || p->nChunks[1] > 0 || p->nWChunks[0] > 0 || p->nWChunks[1] > 0)) {
+      e = cudaMemsetAsync(p->dCounter, 0, 4 * sizeof(unsigned), s);
       if (e != cudaSuccess) { return cudaFail(e, "batch counter clear"); }
    }
    for (int k = 0; k < 2 && rc == MKF_OK; k++) {
@@ -229,16 +233,17 @@ static int planLaunchOn(MKFBatchPlan *p, cudaStream_t s)
       w.tasks = p->dWTasks[k];
       w.chunks = p->dWChunks[k];
       w.nChunks = p->nWChunks[k];
-      w.counter = p->dCounter + 1 + k;
+      w.counter = p->dCounter + k;
       rc = launchWordsBatch(w, k == 0 ? ENC_F32 : ENC_F64, s);
    }
-   if (rc == MKF_OK && p->nChunks > 0) {
+   for (int k = 0; k < 2 && rc == MKF_OK; k++) {
+      if (p->nChunks[k] == 0) { continue; }
       BatchArgs b;
-      b.tasks = p->dTasks;
-      b.chunks = p->dChunks;
-      b.nChunks = p->nChunks;
-      b.counter = p->dCounter;
-      rc = launchThermoBatch(b, s);
+      b.tasks = p->dTasks[k];
+      b.chunks = p->dChunks[k];
+      b.nChunks = p->nChunks[k];
+      b.counter = p->dCounter + 2 + k;
+      rc = launchThermoBatch(b, k == 0 ? ENC_F32 : ENC_F64, p->maxK[k], s);
    }
    for (size_t i = 0; i < p->fallbacks.size() && rc == MKF_OK; i++) {
       const MKFBatchPlan::Fallback &fb = p->fallbacks[i];

@@ -415,9 +415,12 @@ int fieldBPFD(uint64_t *out, const MKFFieldDesc *pF, const MKFThreshSet *pT, int
    const int X = pF->def[0], Y = pF->def[1], Z = pF->def[2];
    if (X < 1 || Y < 1 || Z < 1) { setError("mkfFieldBPFD: bad dimensions %d %d %d", X, Y, Z); return MKF_ERR_ARG; }
    if (!(flags & MKF_F_ACCUMULATE)) {
-      for (int i = 0; i < K; i++) {
-         const int row = rowBase ? rowBase[i] : i;
-         cudaError_t e = cudaMemsetAsync(out + (size_t)row * 256, 0, 256 * sizeof(uint64_t), s);
+      if (!rowBase) {  // rows 0..K-1: one clear
+         cudaError_t e = cudaMemsetAsync(out, 0, (size_t)K * 256 * sizeof(uint64_t), s);
+         if (e != cudaSuccess) { return cudaFail(e, "cudaMemsetAsync"); }
+      }
+      for (int i = 0; rowBase && i < K; i++) {
+         cudaError_t e = cudaMemsetAsync(out + (size_t)rowBase[i] * 256, 0, 256 * sizeof(uint64_t), s);
          if (e != cudaSuccess) { return cudaFail(e, "cudaMemsetAsync"); }
       }
    }

@@ -23,9 +23,10 @@ struct FusedArgs
    double tlo[64];       // sorted thresholds for the "f > t" test, +inf padded
    double thi[64];       // sorted thresholds for the "f >= t" test, +inf padded
    // thermometer kernel: order-preserving 32-bit keys of the thresholds it compares against
-   // (the high word for FP64 fields), sorted, and whether a 2^14-bucket table separates them
+   // (the high word for FP64 fields), sorted, and the most thresholds sharing one bucket of the
+   // 2^14-bucket rank table (1..4; 0 = the table cannot rank these thresholds)
    uint32_t tkey[MKF_MAX_THRESH];
-   int lutOk;
+   int lutC;
 };
 
 
@@ -37,7 +38,8 @@ struct FieldTask
    int X, Y, Z, K, D, nSegX, nTileY, nSlabZ;
    long long nItems;
    uint32_t nanRank;
-   int rankHi, complement, variant;  // variant: 0 f32 >, 1 f32 >=, 2 f64 >, 3 f64 >=; + 4: shifted edge items
+   int rankHi, complement, variant;  // variant: bit 0 ">=", bit 1 FP64, bit 2 shifted edge items, bit 3 lutC > 1
+   int lutC, pad_;
    uint64_t *out;
    int outRow[MKF_MAX_THRESH];
    uint32_t tkey[MKF_MAX_THRESH];
@@ -96,7 +98,9 @@ int planBatchField(const MKFFieldDesc *pF, const MKFThreshSet *pT, int rowBase, 
 
 // Fill a task's key table and item grid; false if its thresholds share a rank-table bucket.
 bool prepareThermoTask(FieldTask &t, int enc);
-int launchThermoBatch(const BatchArgs &b, cudaStream_t s);
+// Launch the batched thermometer kernel over tasks of one element type (enc) whose largest
+// threshold count is maxK.
+int launchThermoBatch(const BatchArgs &b, int enc, int maxK, cudaStream_t s);
 
 // Fill a word task's relation classes, batched variant and item grid (words.cu); launch the
 // batched word kernel over the chunks of tasks of one element type.

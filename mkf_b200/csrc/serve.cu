@@ -154,7 +154,7 @@ struct LaunchSlot
    std::vector<Request *> reqs;
    DevBuf work;      // tasks, chunks, clear list (uploaded each launch)
    DevBuf results;   // counts of requests that want them on the host
-   unsigned *counters = nullptr;  // 3 chunk counters
+   unsigned *counters = nullptr;  // 4 chunk counters: words FP32, FP64, thermometer FP32, FP64
    bool busy = false;
 };
 
@@ -213,8 +213,9 @@ static int issueLaunch(MKFServer *s, LaunchSlot &sl)
       if ((e = cudaStreamWaitEvent(st, sl.copied, 0)) != cudaSuccess) { return cudaFail(e, "server: wait"); }
    }
    // plan every request: word tasks, thermometer tasks, constant maps, single-field fallbacks
-   std::vector<FieldTask> tasks;
-   std::vector<BatchChunk> chunks;
+   std::vector<FieldTask> tasks[2];
+   std::vector<BatchChunk> chunks[2];
+   int maxK[2] = {0, 0};
    std::vector<WordTask> wtasks[2];
    std::vector<BatchChunk> wchunks[2];
    std::vector<ClearEntry> clears;
@@ -255,36 +256,40 @@ static int issueLaunch(MKFServer *s, LaunchSlot &sl)
          w.out = r->dCounts;
          wtasks[k].push_back(w);
       } else if (kind == kPlanThermo) {
-         const int f = (int)tasks.size();
-         for (long long b = 0; b < t.nItems; b += kChunk) { chunks.push_back({f, 0, b, std::min<long long>(b + kChunk, t.nItems)}); }
+         const int k = d.enc == ENC_F32 ? 0 : 1;
+         const int f = (int)tasks[k].size();
+         for (long long b = 0; b < t.nItems; b += kChunk) { chunks[k].push_back({f, 0, b, std::min<long long>(b + kChunk, t.nItems)}); }
          t.out = r->dCounts;
-         tasks.push_back(t);
+         tasks[k].push_back(t);
+         maxK[k] = std::max(maxK[k], t.K);
       }
    }
-   // one upload of the whole work list: [clears][tasks][chunks][wtasks0][wchunks0][wtasks1][wchunks1]
-   auto al = [](size_t n) { return (n + 255) & ~(size_t)255; };
-   size_t off[8];
-   off[0] = 0;
-   off[1] = off[0] + al(clears.size() * sizeof(ClearEntry));
-   off[2] = off[1] + al(tasks.size() * sizeof(FieldTask));
-   off[3] = off[2] + al(chunks.size() * sizeof(BatchChunk));
-   off[4] = off[3] + al(wtasks[0].size() * sizeof(WordTask));
-   off[5] = off[4] + al(wchunks[0].size() * sizeof(BatchChunk));
-   off[6] = off[5] + al(wtasks[1].size() * sizeof(WordTask));
-   off[7] = off[6] + al(wchunks[1].size() * sizeof(BatchChunk));
-   if ((e = sl.work.ensure(off[7])) != cudaSuccess) { return cudaFail(e, "server: work list buffers"); }
+   // one upload of the whole work list, segments 256-byte aligned:
+   // clears | thermometer tasks, chunks (FP32, FP64) | word tasks, chunks (FP32, FP64)
+   struct Seg { const void *src; size_t bytes; size_t off; };
+   Seg seg[9] = {{clears.data(), clears.size() * sizeof(ClearEntry), 0},
+                 {tasks[0].data(), tasks[0].size() * sizeof(FieldTask), 0},
+                 {chunks[0].data(), chunks[0].size() * sizeof(BatchChunk), 0},
+                 {tasks[1].data(), tasks[1].size() * sizeof(FieldTask), 0},
+                 {chunks[1].data(), chunks[1].size() * sizeof(BatchChunk), 0},
+                 {wtasks[0].data(), wtasks[0].size() * sizeof(WordTask), 0},
+                 {wchunks[0].data(), wchunks[0].size() * sizeof(BatchChunk), 0},
+                 {wtasks[1].data(), wtasks[1].size() * sizeof(WordTask), 0},
+                 {wchunks[1].data(), wchunks[1].size() * sizeof(BatchChunk), 0}};
+   size_t total = 0;
+   for (Seg &g : seg) {
+      g.off = total;
+      total += (g.bytes + 255) & ~(size_t)255;
+   }
+   if ((e = sl.work.ensure(total)) != cudaSuccess) { return cudaFail(e, "server: work list buffers"); }
    char *h = (char *)sl.work.h, *dv = (char *)sl.work.d;
-   memcpy(h + off[0], clears.data(), clears.size() * sizeof(ClearEntry));
-   memcpy(h + off[1], tasks.data(), tasks.size() * sizeof(FieldTask));
-   memcpy(h + off[2], chunks.data(), chunks.size() * sizeof(BatchChunk));
-   memcpy(h + off[3], wtasks[0].data(), wtasks[0].size() * sizeof(WordTask));
-   memcpy(h + off[4], wchunks[0].data(), wchunks[0].size() * sizeof(BatchChunk));
-   memcpy(h + off[5], wtasks[1].data(), wtasks[1].size() * sizeof(WordTask));
-   memcpy(h + off[6], wchunks[1].data(), wchunks[1].size() * sizeof(BatchChunk));
-   if ((e = cudaMemcpyAsync(dv, h, off[7], cudaMemcpyHostToDevice, st)) != cudaSuccess) { return cudaFail(e, "server: work list upload"); }
-   if ((e = cudaMemsetAsync(sl.counters, 0, 3 * sizeof(unsigned), st)) != cudaSuccess) { return cudaFail(e, "server: counters"); }
+   for (const Seg &g : seg) {
+      if (g.bytes) { memcpy(h + g.off, g.src, g.bytes); }
+   }
+   if ((e = cudaMemcpyAsync(dv, h, total, cudaMemcpyHostToDevice, st)) != cudaSuccess) { return cudaFail(e, "server: work list upload"); }
+   if ((e = cudaMemsetAsync(sl.counters, 0, 4 * sizeof(unsigned), st)) != cudaSuccess) { return cudaFail(e, "server: counters"); }
    if (!clears.empty()) {
-      clearCounts<<<(unsigned)std::min<size_t>(clears.size(), 1024), 256, 0, st>>>((const ClearEntry *)(dv + off[0]), (int)clears.size());
+      clearCounts<<<(unsigned)std::min<size_t>(clears.size(), 1024), 256, 0, st>>>((const ClearEntry *)(dv + seg[0].off), (int)clears.size());
       if ((e = cudaGetLastError()) != cudaSuccess) { return cudaFail(e, "server: clear launch"); }
    }
    int rc = MKF_OK;
@@ -294,19 +299,20 @@ static int issueLaunch(MKFServer *s, LaunchSlot &sl)
    for (int k = 0; k < 2 && rc == MKF_OK; k++) {
       if (wchunks[k].empty()) { continue; }
       WordBatchArgs w;
-      w.tasks = (const WordTask *)(dv + off[3 + 2 * k]);
-      w.chunks = (const BatchChunk *)(dv + off[4 + 2 * k]);
+      w.tasks = (const WordTask *)(dv + seg[5 + 2 * k].off);
+      w.chunks = (const BatchChunk *)(dv + seg[6 + 2 * k].off);
       w.nChunks = (int)wchunks[k].size();
-      w.counter = sl.counters + 1 + k;
+      w.counter = sl.counters + k;
       rc = launchWordsBatch(w, k == 0 ? ENC_F32 : ENC_F64, st);
    }
-   if (rc == MKF_OK && !chunks.empty()) {
+   for (int k = 0; k < 2 && rc == MKF_OK; k++) {
+      if (chunks[k].empty()) { continue; }
       BatchArgs b;
-      b.tasks = (const FieldTask *)(dv + off[1]);
-      b.chunks = (const BatchChunk *)(dv + off[2]);
-      b.nChunks = (int)chunks.size();
-      b.counter = sl.counters;
-      rc = launchThermoBatch(b, st);
+      b.tasks = (const FieldTask *)(dv + seg[1 + 2 * k].off);
+      b.chunks = (const BatchChunk *)(dv + seg[2 + 2 * k].off);
+      b.nChunks = (int)chunks[k].size();
+      b.counter = sl.counters + 2 + k;
+      rc = launchThermoBatch(b, k == 0 ? ENC_F32 : ENC_F64, maxK[k], st);
    }
    for (size_t i = 0; i < singles.size() && rc == MKF_OK; i++) {
       Request *r = singles[i].r;
@@ -468,7 +474,7 @@ MKF_API int mkfServerCreate(MKFServer **ps, const MKFServerConfig *cfg)
       if (e == cudaSuccess) { e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking); }
       if (e == cudaSuccess) { e = cudaEventCreateWithFlags(&sl.copied, cudaEventDisableTiming); }
       if (e == cudaSuccess) { e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming); }
-      if (e == cudaSuccess) { e = cudaMalloc(&sl.counters, 3 * sizeof(unsigned)); }
+      if (e == cudaSuccess) { e = cudaMalloc(&sl.counters, 4 * sizeof(unsigned)); }
    }
    if (e != cudaSuccess) {
       const int rc = cudaFail(e, "mkfServerCreate");

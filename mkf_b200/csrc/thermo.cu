@@ -33,6 +33,9 @@ static constexpr int kThWarps = 8;
 #ifndef THERMO_MINB
 #define THERMO_MINB (THERMO_TY == 8 ? 3 : 2)
 #endif
+#ifndef THERMO_BATCH_MINB
+#define THERMO_BATCH_MINB 2  // the per-field variant switch needs the larger register budget
+#endif
 static constexpr int kThSlots = 3;  // predicated mixed-code slots per cell (K > 1)
 static constexpr int kLutShift = 18;
 static constexpr int kLutSize = 1 << (32 - kLutShift);
@@ -129,8 +132,8 @@ struct PlaneOnes
 // per-threshold totals. The [K][256] histogram and the warps' staging planes are dynamic.
 struct ThermoShared
 {
-   uint8_t lut[kLutSize];
-   uint32_t key[MKF_MAX_THRESH + 1];
+   alignas(16) uint8_t lut[kLutSize];
+   uint32_t key[MKF_MAX_THRESH + 4];  // padded: a bucket's candidates may run past the last key
    double tlo[64];
    double thi[64];
    uint32_t ones[MKF_MAX_THRESH];
@@ -166,14 +169,24 @@ __device__ void ctaSetup(const P &a, ThermoShared &S, uint32_t *hist)
       S.tlo[i] = a.tlo[i];
       S.thi[i] = a.thi[i];
    }
-   for (int i = threadIdx.x; i <= MKF_MAX_THRESH; i += blockDim.x) { S.key[i] = (i < K) ? a.tkey[i] : 0xFFFFFFFFu; }
+   for (int i = threadIdx.x; i < MKF_MAX_THRESH + 4; i += blockDim.x) { S.key[i] = (i < K) ? a.tkey[i] : 0xFFFFFFFFu; }
    __syncthreads();
-   // bucket b -> number of threshold keys below the bucket's first key
-   for (int b = threadIdx.x; b < kLutSize; b += blockDim.x) {
-      const uint32_t start = (uint32_t)b << kLutShift;
-      uint32_t n = 0;
-      for (int k = 0; k < K; k++) { n += S.key[k] < start; }
-      S.lut[b] = (uint8_t)n;
+   // bucket b -> number of threshold keys below the bucket's first key (keys sorted: binary
+   // search), four buckets per 32-bit store
+   uint32_t *lut4 = reinterpret_cast<uint32_t *>(S.lut);
+   for (int w = threadIdx.x; w < kLutSize / 4; w += blockDim.x) {
+      uint32_t word = 0;
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+         const uint32_t start = (uint32_t)(4 * w + q) << kLutShift;
+         int lo = 0, hi = K;  // first key >= start
+         while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (S.key[mid] < start) { lo = mid + 1; } else { hi = mid; }
+         }
+         word |= (uint32_t)lo << (8 * q);
+      }
+      lut4[w] = word;
    }
    if (threadIdx.x < MKF_MAX_THRESH) { S.ones[threadIdx.x] = 0; }
    if (threadIdx.x == 0) { S.cells = 0; }
@@ -242,7 +255,8 @@ __device__ __forceinline__ uint32_t cellCode(uint32_t R0, uint32_t R1, uint32_t 
 // by `a` into the CTA's histogram and all-ones totals. Returns the item's number of cells.
 // INNER: the field has X >= 32, Y > TY, and a positive row stride whose TY multiple fits 32 bits
 // in bytes. NSLOT: 3 mixed-code slots, or 1 for one threshold (a cell then has at most one).
-template <typename T, int TY, bool GE, int NSLOT, bool INNER, typename P>
+// CMAX: rank-table candidates compared per element (1, or 4 when thresholds share buckets).
+template <typename T, int TY, bool GE, int NSLOT, bool INNER, int CMAX, typename P>
 __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it, ThermoShared &S, uint32_t *sHist)
 {
    static_assert(NSLOT == 1 || NSLOT == 3, "one or three slots");
@@ -302,8 +316,17 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
          const uint32_t r0 = S.lut[key >> kLutShift];
          const uint32_t cand = S.key[r0];
          r[j] = r0 + (GE ? (key >= cand) : (key > cand));
+         bool tie = key == cand;
+#pragma unroll
+         for (int c = 1; c < CMAX; ++c) {
+            // further thresholds of the same bucket; keys of later buckets (or the padding) are
+            // above every key of this bucket and add nothing
+            const uint32_t cc = S.key[r0 + c];
+            r[j] += GE ? (key >= cc) : (key > cc);
+            tie = tie || key == cc;
+         }
          if (W == 2) {
-            slow = slow || key == cand || key >= 0xFFF00000u || key < 0x00100000u;
+            slow = slow || tie || key >= 0xFFF00000u || key < 0x00100000u;
          } else {
             r[j] = ((wj & 0x7FFFFFFFu) > 0x7F800000u) ? nanRank : r[j];
          }
@@ -398,7 +421,7 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
    return (unsigned long long)(xe - xs) * (unsigned)(jhi - jlo) * (unsigned)nPln;
 }
 
-template <typename T, int TY, bool GE, int NSLOT, bool INNER>
+template <typename T, int TY, bool GE, int NSLOT, bool INNER, int CMAX>
 __global__ void __launch_bounds__(kThWarps * 32, THERMO_MINB) thermoBPFD(const __grid_constant__ FusedArgs a)
 {
    __shared__ ThermoShared S;
@@ -407,7 +430,7 @@ __global__ void __launch_bounds__(kThWarps * 32, THERMO_MINB) thermoBPFD(const _
    const long long gw = (long long)blockIdx.x * kThWarps + (threadIdx.x >> 5);
    const long long nw = (long long)gridDim.x * kThWarps;
    unsigned long long cells = 0;
-   for (long long it = gw; it < a.nItems; it += nw) { cells += warpItem<T, TY, GE, NSLOT, INNER>(a, it, S, sHist); }
+   for (long long it = gw; it < a.nItems; it += nw) { cells += warpItem<T, TY, GE, NSLOT, INNER, CMAX>(a, it, S, sHist); }
    if ((threadIdx.x & 31) == 0 && cells) { atomicAdd(&S.cells, cells); }
    ctaFlush(a, S, sHist);
 }
@@ -416,9 +439,10 @@ __global__ void __launch_bounds__(kThWarps * 32, THERMO_MINB) thermoBPFD(const _
 
 // A CTA takes chunks of consecutive work items from a global counter; chunks never span fields.
 // When the next chunk belongs to another field, the CTA adds its counts of the previous field to
-// that field's output rows, then loads the new field's thresholds and rank table.
-template <int TY>
-__global__ void __launch_bounds__(kThWarps * 32, THERMO_MINB) thermoBatch(const __grid_constant__ BatchArgs b)
+// that field's output rows, then loads the new field's thresholds and rank table. One kernel per
+// element type keeps the per-field switch to four variants (relation, shifted edge items).
+template <typename T, int TY>
+__global__ void __launch_bounds__(kThWarps * 32, THERMO_BATCH_MINB) thermoBatch(const __grid_constant__ BatchArgs b)
 {
    __shared__ ThermoShared S;
    __shared__ FieldTask F;
@@ -449,15 +473,15 @@ __global__ void __launch_bounds__(kThWarps * 32, THERMO_MINB) thermoBatch(const 
          cur = ch.field;
       }
       for (long long it = ch.begin + warp; it < ch.end; it += kThWarps) {
-         switch (F.variant) {
-            case 0: cells += warpItem<float, TY, false, kThSlots, false>(F, it, S, sHist); break;
-            case 1: cells += warpItem<float, TY, true, kThSlots, false>(F, it, S, sHist); break;
-            case 2: cells += warpItem<double, TY, false, kThSlots, false>(F, it, S, sHist); break;
-            case 3: cells += warpItem<double, TY, true, kThSlots, false>(F, it, S, sHist); break;
-            case 4: cells += warpItem<float, TY, false, kThSlots, true>(F, it, S, sHist); break;
-            case 5: cells += warpItem<float, TY, true, kThSlots, true>(F, it, S, sHist); break;
-            case 6: cells += warpItem<double, TY, false, kThSlots, true>(F, it, S, sHist); break;
-            default: cells += warpItem<double, TY, true, kThSlots, true>(F, it, S, sHist); break;
+         switch (F.variant & 13) {
+            case 0: cells += warpItem<T, TY, false, kThSlots, false, 1>(F, it, S, sHist); break;
+            case 1: cells += warpItem<T, TY, true, kThSlots, false, 1>(F, it, S, sHist); break;
+            case 4: cells += warpItem<T, TY, false, kThSlots, true, 1>(F, it, S, sHist); break;
+            case 5: cells += warpItem<T, TY, true, kThSlots, true, 1>(F, it, S, sHist); break;
+            case 8: cells += warpItem<T, TY, false, kThSlots, false, 4>(F, it, S, sHist); break;
+            case 9: cells += warpItem<T, TY, true, kThSlots, false, 4>(F, it, S, sHist); break;
+            case 12: cells += warpItem<T, TY, false, kThSlots, true, 4>(F, it, S, sHist); break;
+            default: cells += warpItem<T, TY, true, kThSlots, true, 4>(F, it, S, sHist); break;
          }
       }
    }
@@ -485,12 +509,12 @@ static uint32_t thresholdKey(double t, int enc, bool ge)
    return sortKey(u);
 }
 
-template <typename T, int TY, bool GE, int NSLOT, bool INNER>
+template <typename T, int TY, bool GE, int NSLOT, bool INNER, int CMAX>
 static int launchThermoT(const FusedArgs &a, cudaStream_t s)
 {
    static int blocksPerSMofK[MKF_MAX_THRESH + 1] = {0};
    static bool attr = false;
-   auto kern = thermoBPFD<T, TY, GE, NSLOT, INNER>;
+   auto kern = thermoBPFD<T, TY, GE, NSLOT, INNER, CMAX>;
    if (!attr) {
       // static + dynamic shared memory exceeds the default 48 KB for large K
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)thermoDynBytes(MKF_MAX_THRESH));
@@ -518,17 +542,20 @@ static bool innerTiles(const P &a, int enc)
    return a.X >= 32 && a.Y > THERMO_TY && rowBytes > 0 && rowBytes * THERMO_TY < ((int64_t)1 << 32);
 }
 
-// Fill the key table of a thermometer pass; returns false when two thresholds share a bucket of
-// the rank table (such passes use the binary-search kernel of fused.cu).
+// Fill the key table of a thermometer pass and return the most thresholds sharing one bucket of
+// the rank table (1..4), or 0 when more share one (such passes use the binary-search kernel of
+// fused.cu).
 template <typename P>
-static bool prepareKeys(P &a, int enc)
+static int prepareKeys(P &a, int enc)
 {
    const bool ge = a.rankHi != 0;
    for (int k = 0; k < a.K; k++) { a.tkey[k] = thresholdKey(ge ? a.thi[k] : a.tlo[k], enc, ge); }
-   for (int k = 0; k + 1 < a.K; k++) {
-      if ((a.tkey[k] >> kLutShift) == (a.tkey[k + 1] >> kLutShift)) { return false; }
+   int most = 1, run = 1;
+   for (int k = 1; k < a.K; k++) {
+      run = ((a.tkey[k] >> kLutShift) == (a.tkey[k - 1] >> kLutShift)) ? run + 1 : 1;
+      most = std::max(most, run);
    }
-   return true;
+   return most <= 4 ? most : 0;
 }
 
 // Work-item grid of a field for the thermometer kernels (TY rows, D planes, 31 cells per item).
@@ -545,20 +572,28 @@ static void itemGrid(P &a, int D)
 
 bool prepareThermoTask(FieldTask &t, int enc)
 {
-   t.variant = (enc == ENC_F32 ? 0 : 2) + (t.rankHi ? 1 : 0) + (innerTiles(t, enc) ? 4 : 0);
-   if (!prepareKeys(t, enc)) { return false; }
+   t.lutC = prepareKeys(t, enc);
+   if (t.lutC == 0) { return false; }
+   t.variant = (enc == ENC_F32 ? 0 : 2) + (t.rankHi ? 1 : 0) + (innerTiles(t, enc) ? 4 : 0) + (t.lutC > 1 ? 8 : 0);
    itemGrid(t, 32);
    return true;
 }
 
-int launchThermoBatch(const BatchArgs &b, cudaStream_t s)
+int launchThermoBatch(const BatchArgs &b, int enc, int maxK, cudaStream_t s)
 {
    constexpr int TY = THERMO_TY;
-   static int blocksPerSM = -1;
-   auto kern = thermoBatch<TY>;
-   const size_t smem = thermoDynBytes(MKF_MAX_THRESH);
-   if (blocksPerSM < 0) {
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+   static int blocksPerSMofK[2][MKF_MAX_THRESH + 1] = {};
+   static bool attr[2] = {false, false};
+   const int e = enc == ENC_F32 ? 0 : 1;
+   auto kern = e == 0 ? thermoBatch<float, TY> : thermoBatch<double, TY>;
+   if (maxK < 1 || maxK > MKF_MAX_THRESH) { setError("thermoBatch: bad threshold count %d", maxK); return MKF_ERR_ARG; }
+   const size_t smem = thermoDynBytes(maxK);  // every field of the batch has at most maxK thresholds
+   if (!attr[e]) {
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)thermoDynBytes(MKF_MAX_THRESH));
+      attr[e] = true;
+   }
+   int &blocksPerSM = blocksPerSMofK[e][maxK];
+   if (blocksPerSM <= 0) {
       int n = 0;
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, kThWarps * 32, smem);
       blocksPerSM = n > 0 ? n : 1;
@@ -574,15 +609,18 @@ template <typename T, bool GE>
 static int launchThermoG(const FusedArgs &a, bool inner, cudaStream_t s)
 {
    constexpr int TY = THERMO_TY;
-   // one threshold: a cell has at most one mixed code
-   if (a.K == 1) { return inner ? launchThermoT<T, TY, GE, 1, true>(a, s) : launchThermoT<T, TY, GE, 1, false>(a, s); }
-   return inner ? launchThermoT<T, TY, GE, kThSlots, true>(a, s) : launchThermoT<T, TY, GE, kThSlots, false>(a, s);
+   // one threshold: a cell has at most one mixed code (and the rank table one candidate)
+   if (a.K == 1) { return inner ? launchThermoT<T, TY, GE, 1, true, 1>(a, s) : launchThermoT<T, TY, GE, 1, false, 1>(a, s); }
+   if (a.lutC > 1) {
+      return inner ? launchThermoT<T, TY, GE, kThSlots, true, 4>(a, s) : launchThermoT<T, TY, GE, kThSlots, false, 4>(a, s);
+   }
+   return inner ? launchThermoT<T, TY, GE, kThSlots, true, 1>(a, s) : launchThermoT<T, TY, GE, kThSlots, false, 1>(a, s);
 }
 
 int launchThermo(FusedArgs &a, int enc, cudaStream_t s)
 {
-   a.lutOk = prepareKeys(a, enc) ? 1 : 0;
-   if (!a.lutOk) { return MKF_ERR_UNSUPPORTED; }
+   a.lutC = prepareKeys(a, enc);
+   if (a.lutC == 0) { return MKF_ERR_UNSUPPORTED; }
    itemGrid(a, 32);
    const bool ge = a.rankHi != 0, inner = innerTiles(a, enc);
    if (enc == ENC_F32) { return ge ? launchThermoG<float, true>(a, inner, s) : launchThermoG<float, false>(a, inner, s); }

@@ -406,3 +406,34 @@ def test_slab_shards_sum_to_whole_field(mkf, oracle, cuda):
             z0, z1 = slab_planes(50, world, r)
             tot += u64(sharded_field_bpfd(fd[z0:z1], t, 4))
         assert (tot == want).all(), world
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_thresholds_sharing_rank_table_buckets(mkf, oracle, cuda, dtype):
+    """Thresholds closer than a rank-table bucket (2 to 4 per bucket, duplicates; 5 per bucket
+    takes the general kernel), elements on and between them, single-field and batched."""
+    import torch
+
+    rng = np.random.default_rng(17)
+    sets = [
+        [0.5, 0.5001, 0.52, 0.6, -1.0, 2.0],               # four in [0.5, 0.625)
+        [1.0, 1.0, 1.1, 1.2, 3.0],                          # a duplicate and three in one bucket
+        [0.25, 0.26, 0.27, 0.28, 0.29, -0.5],               # five in one bucket: general kernel
+        list(np.linspace(-0.3, 0.3, 16)),
+    ]
+    fields, ths = [], []
+    for i, t in enumerate(sets):
+        shape = (int(rng.integers(20, 40)), int(rng.integers(30, 70)), int(rng.integers(33, 90)))
+        f = rng.choice(np.asarray(t + [0.0, 0.55, 1.05, 0.255], dtype=dtype), size=shape)
+        f = f + (rng.integers(-2, 3, size=shape) * 0.01).astype(dtype) * (rng.random(shape) < 0.5)
+        f = f.astype(dtype)
+        Z, Y, X = shape
+        for m in (mkf.BMC_GT, mkf.BMC_GT | mkf.BMC_EQ, mkf.BMC_LT):
+            got = u64(mkf.field_bpfd(to_dev(f, cuda), t, m))
+            assert (got == oracle.bpfd_field(f, (X, Y, Z), t, m)).all(), (i, m)
+        fields.append(to_dev(f, cuda))
+        ths.append(t)
+    plan = mkf.BatchPlan(fields, ths)
+    want = np.concatenate([u64(mkf.field_bpfd(f, t, mkf.BMC_GT)) for f, t in zip(fields, ths)])
+    assert (u64(plan.launch()) == want).all()
+    plan.close()
