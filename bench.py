@@ -290,6 +290,8 @@ def run_serving_workload(dev, rates=(100, 500, 1000, 2000, 5000), max_requests=1
     stream(requests(200), 0)  # warm-up
     per_rate = [stream(requests(int(min(max_requests, r * seconds))), r) for r in rates]
     burst = stream(requests(2000), 0)
+    dev_only = [r for r in requests(6000) if pool[r[0]].is_cuda][:2000]
+    burst_dev = stream(dev_only, 0)
 
     # the plain per-field call on a sample of the same mix: host fields copied first, then one
     # binMapCUDA + mkfCUDAGetBPFDH per threshold, as a caller of the original library would
@@ -311,6 +313,9 @@ def run_serving_workload(dev, rates=(100, 500, 1000, 2000, 5000), max_requests=1
         "per_rate": per_rate,
         "saturated_fields_per_s": burst["fields_per_s"],
         "saturated_h2d_gb_per_s": burst["h2d_gb_per_s"],
+        "saturated_device_resident_fields_per_s": burst_dev["fields_per_s"],
+        "saturated_device_resident_gvoxel_per_s": burst_dev["gvoxel_per_s"],
+        "saturated_device_resident_p99_ms": burst_dev["p99_ms"],
         "bound": "host-to-device copies of the pinned-host half of the requests (PCIe) at saturation",
         "saturated_p99_ms": burst["p99_ms"],
         "plain_dropin_fields_per_s": plain,
