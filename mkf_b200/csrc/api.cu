@@ -46,19 +46,26 @@ __global__ void measuresKernel(double *r, const uint64_t *h, int nSets)
    r[4 * i + 3] = (double)k / 24.0;
 }
 
-static std::once_flag gConstOnce;
-static int gConstRc = MKF_OK;
+// __constant__ memory belongs to each device: upload the tables once per device, on first use
+// with that device current.
+static std::mutex gConstMu;
+static bool gConstDone[64] = {};
 
 static int uploadConstants()
 {
-   std::call_once(gConstOnce, [] {
-      cudaError_t e = cudaMemcpyToSymbol(cGroupOf, kGroupOf, sizeof(cGroupOf));
-      if (e == cudaSuccess) { e = cudaMemcpyToSymbol(cWK, kWK, sizeof(cWK)); }
-      if (e == cudaSuccess) { e = cudaMemcpyToSymbol(cWS, kWS, sizeof(cWS)); }
-      if (e == cudaSuccess) { e = cudaMemcpyToSymbol(cWM, kWM, sizeof(cWM)); }
-      gConstRc = cudaFail(e, "measure constants upload");
-   });
-   return gConstRc;
+   int dev = 0;
+   cudaError_t e = cudaGetDevice(&dev);
+   if (e != cudaSuccess) { return cudaFail(e, "cudaGetDevice"); }
+   if (dev < 0 || dev >= 64) { setError("measure constants: device %d out of range", dev); return MKF_ERR_UNSUPPORTED; }
+   std::lock_guard<std::mutex> lk(gConstMu);
+   if (gConstDone[dev]) { return MKF_OK; }
+   e = cudaMemcpyToSymbol(cGroupOf, kGroupOf, sizeof(cGroupOf));
+   if (e == cudaSuccess) { e = cudaMemcpyToSymbol(cWK, kWK, sizeof(cWK)); }
+   if (e == cudaSuccess) { e = cudaMemcpyToSymbol(cWS, kWS, sizeof(cWS)); }
+   if (e == cudaSuccess) { e = cudaMemcpyToSymbol(cWM, kWM, sizeof(cWM)); }
+   if (e != cudaSuccess) { return cudaFail(e, "measure constants upload"); }
+   gConstDone[dev] = true;
+   return MKF_OK;
 }
 
 // Device buffers reused by the host-field path (grown on demand, guarded by a mutex).

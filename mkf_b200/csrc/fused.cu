@@ -252,15 +252,10 @@ static int levelsFor(int K)
 template <typename T, int LEVELS, int TY, bool THERMO>
 static int launchFused(const FusedArgs &a, cudaStream_t s)
 {
-   static int blocksPerSM = -1;
+   static std::atomic<int> occ{0};
    const size_t smem = (size_t)a.K * 256 * sizeof(uint32_t);
    auto kern = fusedBPFD<T, LEVELS, TY, THERMO>;
-   if (blocksPerSM < 0) {
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, MKF_MAX_THRESH * 256 * 4);
-      int n = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, kWarps * 32, MKF_MAX_THRESH * 256 * 4);
-      blocksPerSM = n > 0 ? n : 1;
-   }
+   const int blocksPerSM = cachedOccupancy(occ, kern, kWarps * 32, MKF_MAX_THRESH * 256 * 4, MKF_MAX_THRESH * 256 * 4);
    long long grid = ((long long)a.nItems + kWarps - 1) / kWarps;
    const long long cap = (long long)smCount() * blocksPerSM;
    if (grid > cap) { grid = cap; }

@@ -1,5 +1,6 @@
 // mkf_common.cuh - shared host/device helpers of libMKF.so (sm_100a).
 #pragma once
+#include <atomic>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stddef.h>
@@ -15,6 +16,22 @@ void setError(const char *fmt, ...);
 // Record a CUDA error as the last error; returns MKF_ERR_CUDA when e != cudaSuccess.
 int cudaFail(cudaError_t e, const char *what);
 int smCount();
+
+// Resident CTAs per SM of `kern` for a block size and dynamic shared-memory size, computed on the
+// first call for a cache slot and kept there (a relaxed atomic: host threads that race compute the
+// same value). maxSmem > 48 KB is first allowed with cudaFuncSetAttribute.
+template <typename K>
+int cachedOccupancy(std::atomic<int> &slot, K kern, int threads, size_t smem, size_t maxSmem = 0)
+{
+   int v = slot.load(std::memory_order_relaxed);
+   if (v > 0) { return v; }
+   if (maxSmem > 48 * 1024) { cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)maxSmem); }
+   int n = 0;
+   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, threads, smem);
+   v = n > 0 ? n : 1;
+   slot.store(v, std::memory_order_relaxed);
+   return v;
+}
 // Log a message on stderr the way the original library reports CUDA failures (ctuErr).
 void logError(const char *fmt, ...);
 

@@ -512,20 +512,9 @@ static uint32_t thresholdKey(double t, int enc, bool ge)
 template <typename T, int TY, bool GE, int NSLOT, bool INNER, int CMAX>
 static int launchThermoT(const FusedArgs &a, cudaStream_t s)
 {
-   static int blocksPerSMofK[MKF_MAX_THRESH + 1] = {0};
-   static bool attr = false;
+   static std::atomic<int> occ[MKF_MAX_THRESH + 1];  // resident CTAs for each K's histogram size
    auto kern = thermoBPFD<T, TY, GE, NSLOT, INNER, CMAX>;
-   if (!attr) {
-      // static + dynamic shared memory exceeds the default 48 KB for large K
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)thermoDynBytes(MKF_MAX_THRESH));
-      attr = true;
-   }
-   int &blocksPerSM = blocksPerSMofK[a.K];  // resident CTAs for this K's histogram size
-   if (blocksPerSM <= 0) {
-      int n = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, kThWarps * 32, thermoDynBytes(a.K));
-      blocksPerSM = n > 0 ? n : 1;
-   }
+   const int blocksPerSM = cachedOccupancy(occ[a.K], kern, kThWarps * 32, thermoDynBytes(a.K), thermoDynBytes(MKF_MAX_THRESH));
    long long grid = (a.nItems + kThWarps - 1) / kThWarps;
    const long long cap = (long long)smCount() * blocksPerSM;
    if (grid > cap) { grid = cap; }
@@ -582,22 +571,12 @@ bool prepareThermoTask(FieldTask &t, int enc)
 int launchThermoBatch(const BatchArgs &b, int enc, int maxK, cudaStream_t s)
 {
    constexpr int TY = THERMO_TY;
-   static int blocksPerSMofK[2][MKF_MAX_THRESH + 1] = {};
-   static bool attr[2] = {false, false};
+   static std::atomic<int> occ[2][MKF_MAX_THRESH + 1];
    const int e = enc == ENC_F32 ? 0 : 1;
    auto kern = e == 0 ? thermoBatch<float, TY> : thermoBatch<double, TY>;
    if (maxK < 1 || maxK > MKF_MAX_THRESH) { setError("thermoBatch: bad threshold count %d", maxK); return MKF_ERR_ARG; }
    const size_t smem = thermoDynBytes(maxK);  // every field of the batch has at most maxK thresholds
-   if (!attr[e]) {
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)thermoDynBytes(MKF_MAX_THRESH));
-      attr[e] = true;
-   }
-   int &blocksPerSM = blocksPerSMofK[e][maxK];
-   if (blocksPerSM <= 0) {
-      int n = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, kThWarps * 32, smem);
-      blocksPerSM = n > 0 ? n : 1;
-   }
+   const int blocksPerSM = cachedOccupancy(occ[e][maxK], kern, kThWarps * 32, smem, thermoDynBytes(MKF_MAX_THRESH));
    long long grid = (long long)smCount() * blocksPerSM;
    if (grid > b.nChunks) { grid = b.nChunks; }
    if (grid < 1) { grid = 1; }

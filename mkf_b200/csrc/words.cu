@@ -217,13 +217,9 @@ __global__ void __launch_bounds__(kWdWarps * 32, MINB) wordBPFD(const __grid_con
 template <typename T, int KMAX, int CLS0, int CLS1, bool INNER>
 static int launchWordsI(const WordTask &a, cudaStream_t s)
 {
-   static int blocksPerSM = -1;
+   static std::atomic<int> occ{0};
    auto kern = wordBPFD<T, KMAX, CLS0, CLS1, INNER, (INNER && sizeof(T) == 4) ? WORDS_MINB_F32 : 2>;
-   if (blocksPerSM < 0) {
-      int n = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, kWdWarps * 32, 0);
-      blocksPerSM = n > 0 ? n : 1;
-   }
+   const int blocksPerSM = cachedOccupancy(occ, kern, kWdWarps * 32, 0);
    long long grid = (a.nItems + kWdWarps - 1) / kWdWarps;
    const long long cap = (long long)smCount() * blocksPerSM;
    if (grid > cap) { grid = cap; }
@@ -385,15 +381,11 @@ void prepareWordTask(WordTask &a, int enc)
 
 int launchWordsBatch(const WordBatchArgs &b, int enc, cudaStream_t s)
 {
-   static int blocksPerSM[2] = {-1, -1};
+   static std::atomic<int> occ[2];
    const int e = enc == ENC_F32 ? 0 : 1;
    auto kern = e == 0 ? wordBatch<float, 3> : wordBatch<double, 2>;
-   if (blocksPerSM[e] < 0) {
-      int n = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, kWdWarps * 32, 0);
-      blocksPerSM[e] = n > 0 ? n : 1;
-   }
-   long long grid = (long long)smCount() * blocksPerSM[e];
+   const int blocksPerSM = cachedOccupancy(occ[e], kern, kWdWarps * 32, 0);
+   long long grid = (long long)smCount() * blocksPerSM;
    if (grid > b.nChunks) { grid = b.nChunks; }
    if (grid < 1) { grid = 1; }
    kern<<<(unsigned)grid, kWdWarps * 32, 0, s>>>(b);
