@@ -93,7 +93,7 @@ def grf_numpy(nz, ny, nx, seed):
     W *= np.exp(-0.5 * SIGMA * SIGMA * kz * kz)[:, None, None]
     W *= np.exp(-0.5 * SIGMA * SIGMA * ky * ky)[None, :, None]
     W *= np.exp(-0.5 * SIGMA * SIGMA * kx * kx)[None, None, :]
-    f = np.fft.irfftn(W, s=(nz, ny, nx))
+    f = np.fft.irfftn(W, s=(nz, ny, nx), axes=(0, 1, 2))
     f -= f.mean()
     f /= f.std()
     return np.ascontiguousarray(f.ravel())
