@@ -495,7 +495,10 @@ int fieldBPFD(uint64_t *out, const MKFFieldDesc *pF, const MKFThreshSet *pT, int
          a.nanRank = (eqBit != (ps.complement != 0)) ? (uint32_t)a.K : 0u;
       }
       a.out = out;
-      if (a.K <= 2) {
+      // a few thresholds of one relation: one ballot per row and threshold costs less than the
+      // rank table up to 5 (FP32) / 6 (FP64) thresholds (B200, 512^3 Gaussian field)
+      const int wordMaxK = std::min(kWordMaxK, pF->enc == ENC_F32 ? 5 : 6);
+      if (a.K <= 2 || (ps.thermo && a.K <= wordMaxK)) {
          uint32_t masks[MKF_MAX_THRESH];
          for (int k = 0; k < a.K; k++) { masks[k] = ps.mask[idx[k]]; }
          rc = launchWords(a, pF->enc, masks, s);

@@ -46,17 +46,24 @@ struct FieldTask
    double tlo[64], thi[64];
 };
 
-// One field for the word-parallel kernels (one or two thresholds of any relation).
+// Most thresholds the word-parallel kernels take in one read (more than two only when they share
+// one relation < <= > >=).
+#ifndef WORDS_MAX_K
+#define WORDS_MAX_K 6
+#endif
+constexpr int kWordMaxK = WORDS_MAX_K;
+
+// One field for the word-parallel kernels.
 struct WordTask
 {
    const void *f;
    int64_t sx, sy, sz;    // element strides
    int X, Y, Z;
-   int K;                 // 1 or 2
-   int cls[2];            // relation class per threshold (words.cu)
-   uint32_t m[2];         // relation masks
-   double tlo[2], thi[2]; // exact-equivalent thresholds for "f > t" / "f >= t" tests
-   int outRow[2];
+   int K;                 // 1 .. kWordMaxK
+   int cls[kWordMaxK];    // relation class per threshold (words.cu)
+   uint32_t m[kWordMaxK]; // relation masks
+   double tlo[kWordMaxK], thi[kWordMaxK];  // exact-equivalent thresholds for "f > t" / "f >= t" tests
+   int outRow[kWordMaxK];
    int complement;        // the map is counted negated: code c is stored in bin 255 - c
    int variant;           // batched kernel: which instantiation counts this field
    uint64_t *out;
@@ -107,8 +114,9 @@ int launchThermoBatch(const BatchArgs &b, int enc, int maxK, cudaStream_t s);
 void prepareWordTask(WordTask &a, int enc);
 int launchWordsBatch(const WordBatchArgs &b, int enc, cudaStream_t s);
 
-// Word-parallel kernel for one or two thresholds of any relations (words.cu); `masks` are the
-// relation masks of f's (sorted) thresholds. MKF_ERR_UNSUPPORTED for other K.
+// Word-parallel kernel for one or two thresholds of any relations, or up to kWordMaxK thresholds of
+// one relation (words.cu); `masks` are the relation masks of f's (sorted) thresholds.
+// MKF_ERR_UNSUPPORTED otherwise.
 int launchWords(const FusedArgs &f, int enc, const uint32_t *masks, cudaStream_t s);
 
 // Launch the thermometer kernel for a pass whose thresholds all share one relation

@@ -218,7 +218,7 @@ template <typename T, int KMAX, int CLS0, int CLS1, bool INNER>
 static int launchWordsI(const WordTask &a, cudaStream_t s)
 {
    static std::atomic<int> occ{0};
-   auto kern = wordBPFD<T, KMAX, CLS0, CLS1, INNER, (INNER && sizeof(T) == 4) ? WORDS_MINB_F32 : 2>;
+   auto kern = wordBPFD<T, KMAX, CLS0, CLS1, INNER, (INNER && sizeof(T) == 4) ? (KMAX <= 2 ? WORDS_MINB_F32 : 3) : 2>;
    const int blocksPerSM = cachedOccupancy(occ, kern, kWdWarps * 32, 0);
    long long grid = (a.nItems + kWdWarps - 1) / kWdWarps;
    const long long cap = (long long)smCount() * blocksPerSM;
@@ -236,9 +236,34 @@ static int launchWordsT(const WordTask &a, cudaStream_t s)
    return inner ? launchWordsI<T, KMAX, CLS0, CLS1, true>(a, s) : launchWordsI<T, KMAX, CLS0, CLS1, false>(a, s);
 }
 
+// 3 .. kWordMaxK thresholds of one relation class CLS.
+template <typename T, int CLS>
+static int dispatchK(const WordTask &a, cudaStream_t s)
+{
+   switch (a.K) {
+      case 3: return launchWordsT<T, 3, CLS, CLS>(a, s);
+      case 4: return launchWordsT<T, 4, CLS, CLS>(a, s);
+#if WORDS_MAX_K >= 5
+      case 5: return launchWordsT<T, 5, CLS, CLS>(a, s);
+#endif
+#if WORDS_MAX_K >= 6
+      case 6: return launchWordsT<T, 6, CLS, CLS>(a, s);
+#endif
+      default: setError("word kernel: %d thresholds", a.K); return MKF_ERR_UNSUPPORTED;
+   }
+}
+
 template <typename T>
 static int dispatchWords(const WordTask &a, cudaStream_t s)
 {
+   if (a.K > 2) {  // one relation for all (checked by launchWords)
+      switch (a.cls[0]) {
+         case kGT: return dispatchK<T, kGT>(a, s);
+         case kGE: return dispatchK<T, kGE>(a, s);
+         case kLT: return dispatchK<T, kLT>(a, s);
+         default: return dispatchK<T, kLE>(a, s);
+      }
+   }
    if (a.K == 2) {
       if (a.cls[0] == a.cls[1]) {
          switch (a.cls[0]) {
@@ -264,7 +289,7 @@ static int dispatchWords(const WordTask &a, cudaStream_t s)
 // outRow). Returns MKF_ERR_UNSUPPORTED for other K.
 int launchWords(const FusedArgs &f, int enc, const uint32_t *masks, cudaStream_t s)
 {
-   if (f.K < 1 || f.K > 2) { return MKF_ERR_UNSUPPORTED; }
+   if (f.K < 1 || f.K > kWordMaxK) { return MKF_ERR_UNSUPPORTED; }
    WordTask a;
    memset(&a, 0, sizeof(a));
    a.f = f.f;
@@ -279,6 +304,11 @@ int launchWords(const FusedArgs &f, int enc, const uint32_t *masks, cudaStream_t
       a.tlo[k] = f.tlo[k];
       a.thi[k] = f.thi[k];
       a.outRow[k] = f.outRow[k];
+   }
+   if (f.K > 2) {  // more than two thresholds: one relation < <= > >= for all
+      for (int k = 0; k < f.K; k++) {
+         if (a.cls[k] != a.cls[0] || a.cls[k] == kGEN) { return MKF_ERR_UNSUPPORTED; }
+      }
    }
    a.nChunkX = (a.X - 1 + 30) / 31;
    a.nTileY = (a.Y - 1 + 30) / 31;
