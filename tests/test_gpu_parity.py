@@ -437,3 +437,19 @@ def test_thresholds_sharing_rank_table_buckets(mkf, oracle, cuda, dtype):
     want = np.concatenate([u64(mkf.field_bpfd(f, t, mkf.BMC_GT)) for f, t in zip(fields, ths)])
     assert (u64(plan.launch()) == want).all()
     plan.close()
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_three_to_six_thresholds_of_one_relation(mkf, oracle, cuda, dtype):
+    """3..6 thresholds sharing one relation take the word kernel (several map words per row):
+    every relation, ties and NaN, fields narrower and wider than a 32 x 32 tile."""
+    rng = np.random.default_rng(23)
+    for shape in [(7, 20, 45), (5, 40, 70), (9, 33, 100)]:
+        f = (rng.integers(-8, 9, size=shape) * 0.25).astype(dtype)
+        f.ravel()[rng.choice(f.size, f.size // 40, replace=False)] = np.nan
+        Z, Y, X = shape
+        for K in (3, 4, 5, 6):
+            t = list(np.round(rng.uniform(-1.5, 1.5, size=K) * 4) / 4)  # on the value grid: ties
+            for m in (mkf.BMC_GT, mkf.BMC_GT | mkf.BMC_EQ, mkf.BMC_LT, mkf.BMC_LT | mkf.BMC_EQ):
+                got = u64(mkf.field_bpfd(to_dev(f, cuda), t, m))
+                assert (got == oracle.bpfd_field(f, (X, Y, Z), t, m)).all(), (shape, K, m)
