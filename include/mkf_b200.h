@@ -158,7 +158,9 @@ int mkfServerCopyCounts(MKFServer *server, uint64_t ticket, uint64_t *dst, void 
 /* Forget a finished ticket and free its device counts. */
 int mkfServerRelease(MKFServer *server, uint64_t ticket);
 int mkfServerStats(MKFServer *server, MKFServerStats *stats, int reset);
-/* Finishes every submitted request, then frees the server (tickets become invalid). */
+/* Finishes every submitted request, then frees the server (tickets become invalid). Requests that
+ * can no longer be admitted because the budget is held by counts never released fail with
+ * MKF_ERR_BUSY instead of waiting. */
 int mkfServerDestroy(MKFServer *server);
 
 /* ---- measures (closest original: mkfSelectMeasuresBPFD, mkfUtil.c:94) ---- */

@@ -426,6 +426,16 @@ static void workerLoop(MKFServer *s)
                r->state = kRunning;
                sl->reqs.push_back(r);
             }
+            if (s->stop && sl->reqs.empty() && !s->slots[0].busy && !s->slots[1].busy) {
+               // shutting down, nothing in flight and the head still does not fit: the memory is
+               // held by counts the client never released, so the rest can never be admitted
+               while (!pending.empty()) {
+                  finishRequest(s, pending.front(), MKF_ERR_BUSY, "server: shut down before the request fitted the budget");
+                  s->failed++;
+                  pending.pop_front();
+               }
+               anyDone = true;
+            }
             if (anyDone) { s->cvDone.notify_all(); }
             if (!sl->reqs.empty()) {
                sl->busy = true;

@@ -124,3 +124,25 @@ def test_server_budget_admission(mkf, cuda):
         assert st["failed"] == 1 and st["deviceBytesInUse"] == 0
     finally:
         srv.close()
+
+
+def test_server_shutdown_with_unreleased_counts(mkf, cuda):
+    """Counts the client never releases keep their budget; closing the server must not wait for
+    requests that can no longer fit."""
+    import threading
+
+    import torch
+
+    f = torch.randn((20, 30, 40), device=cuda)
+    t = list(np.linspace(-1, 1, 32))  # 32 x 256 x 8 B = 64 KiB of counts per request
+    srv = mkf.Server(hbm_budget=1 << 20)
+    tks = [srv.submit(f, t, mkf.BMC_GT) for _ in range(20)]
+    for tk in tks[:16]:  # 16 x 64 KiB fill the 1 MiB budget
+        srv.wait(tk, timeout=60)
+    with pytest.raises(mkf.MKFError, match="TIMEOUT"):
+        srv.wait(tks[16], timeout=0.5)
+    done = threading.Event()
+    th = threading.Thread(target=lambda: (srv.close(), done.set()))
+    th.start()
+    th.join(timeout=60)
+    assert done.is_set(), "server shutdown waited for requests that cannot fit"
