@@ -69,6 +69,14 @@ const char *mkfLastError(void);
  * uint64_t[nT][256]). */
 int mkfFieldBPFD(uint64_t *pBPFD, const MKFFieldDesc *pF, const MKFThreshSet *pT, int flags, void *stream);
 
+/* The same for one or two thresholds of any relations, with the field's descriptive moments from
+ * the same read (the original declares them as the categorical CUDAImgMom, binMapCUDA.cuh:67-128,
+ * without calling it): pMom (device, double[nT][2][2]) receives per threshold and per map value
+ * (0, 1) the sum of f and the sum of f^2 over the elements, in FP64 (summation order is not fixed,
+ * so results may differ in the last bits between runs). Dimensions must be >= 2 each. */
+int mkfFieldBPFDMoments(uint64_t *pBPFD, double *pMom, const MKFFieldDesc *pF, const MKFThreshSet *pT, int flags,
+                        void *stream);
+
 /* The same from a HOST field: the field is copied in slabs through device staging buffers on a
  * copy stream overlapped with the counting kernel, and the counts are copied back to pBPFDH
  * (host, uint64_t[nT][256]). Synchronous. pF->p may be pageable or pinned host memory. */

@@ -20,7 +20,7 @@ from ._lib import (BMC_AL, BMC_EQ, BMC_GT, BMC_LT, ENC_F32, ENC_F64, MKF_F_ACCUM
                    MKFServerStats, MKFThreshSet, check, lib)
 
 __all__ = [
-    "build", "lib", "MKFError", "BatchPlan", "Server", "relation_mask", "field_bpfd", "field_bpfd_host", "batch_bpfd",
+    "build", "lib", "MKFError", "BatchPlan", "Server", "relation_mask", "field_bpfd", "field_bpfd_moments", "field_bpfd_host", "batch_bpfd",
     "bin_map_cuda", "get_bpfd", "get_bpfd_host", "measures", "measures_dev", "select_measures",
     "ENC_F32", "ENC_F64", "BMC_LT", "BMC_EQ", "BMC_GT", "BMC_AL",
 ]
@@ -110,6 +110,21 @@ def field_bpfd(field, thresholds, mask=BMC_GT, out=None, accumulate=False, strea
                             MKF_F_ACCUMULATE if accumulate else 0, _stream_ptr(stream))
     check(rc, "mkfFieldBPFD")
     return out
+
+
+def field_bpfd_moments(field, thresholds, mask=BMC_GT, stream=None):
+    """Pattern counts of a CUDA field for one or two thresholds together with, from the same read,
+    per threshold and map value the sum of f and of f^2 (FP64). Returns (counts (K, 256) int64,
+    moments (K, 2, 2) float64), both CUDA tensors."""
+    torch = _torch()
+    th = _Thresholds(thresholds, mask)
+    out = torch.zeros((th.n, 256), dtype=torch.int64, device=field.device)
+    mom = torch.zeros((th.n, 2, 2), dtype=torch.float64, device=field.device)
+    strides = None if field.is_contiguous() else field.stride()
+    d = _field_desc(field.data_ptr(), _enc_of(field), field.shape, strides)
+    check(lib().mkfFieldBPFDMoments(out.data_ptr(), mom.data_ptr(), C.byref(d), C.byref(th.ts), 0, _stream_ptr(stream)),
+          "mkfFieldBPFDMoments")
+    return out, mom
 
 
 def field_bpfd_host(field: np.ndarray, thresholds, mask=BMC_GT) -> np.ndarray:

@@ -121,6 +121,7 @@ _SIG = [
     ("sumNI", C.c_int, [C.POINTER(C.c_int), C.c_int]),
     ("mkfLastError", C.c_char_p, []),
     ("mkfFieldBPFD", C.c_int, [_P, C.POINTER(MKFFieldDesc), C.POINTER(MKFThreshSet), C.c_int, _P]),
+    ("mkfFieldBPFDMoments", C.c_int, [_P, _P, C.POINTER(MKFFieldDesc), C.POINTER(MKFThreshSet), C.c_int, _P]),
     ("mkfFieldBPFDHost", C.c_int, [_P, C.POINTER(MKFFieldDesc), C.POINTER(MKFThreshSet)]),
     ("mkfFieldBPFDHostNoAlloc", C.c_int, [_P, C.POINTER(MKFFieldDesc), C.POINTER(MKFThreshSet), _P]),
     ("mkfBatchPlanCreate", C.c_int, [C.POINTER(C.c_void_p), _P, C.POINTER(MKFFieldDesc), C.POINTER(MKFThreshSet), C.c_int]),

@@ -89,6 +89,42 @@ MKF_API int mkfFieldBPFD(uint64_t *pBPFD, const MKFFieldDesc *pF, const MKFThres
    return fieldBPFD(pBPFD, pF, pT, flags, (cudaStream_t)stream, nullptr);
 }
 
+MKF_API int mkfFieldBPFDMoments(uint64_t *pBPFD, double *pMom, const MKFFieldDesc *pF, const MKFThreshSet *pT,
+                                int flags, void *stream)
+{
+   if (!pBPFD || !pMom || !pF || !pT || !pF->p || !pT->t) { setError("mkfFieldBPFDMoments: NULL argument"); return MKF_ERR_ARG; }
+   const int K = pT->nT;
+   if (K < 1 || K > 2) { setError("mkfFieldBPFDMoments: nT=%d, moments are counted for 1 or 2 thresholds", K); return MKF_ERR_UNSUPPORTED; }
+   if (pF->enc != ENC_F32 && pF->enc != ENC_F64) { setError("mkfFieldBPFDMoments: encoding 0x%02X not supported", pF->enc); return MKF_ERR_UNSUPPORTED; }
+   const int X = pF->def[0], Y = pF->def[1], Z = pF->def[2];
+   if (X < 2 || Y < 2 || Z < 2) { setError("mkfFieldBPFDMoments: dimensions %d %d %d (each must be >= 2)", X, Y, Z); return MKF_ERR_ARG; }
+   cudaStream_t s = (cudaStream_t)stream;
+   if (!(flags & MKF_F_ACCUMULATE)) {
+      cudaError_t e = cudaMemsetAsync(pBPFD, 0, (size_t)K * 256 * sizeof(uint64_t), s);
+      if (e == cudaSuccess) { e = cudaMemsetAsync(pMom, 0, (size_t)K * 4 * sizeof(double), s); }
+      if (e != cudaSuccess) { return cudaFail(e, "cudaMemsetAsync"); }
+   }
+   FusedArgs a;
+   memset(&a, 0, sizeof(a));
+   a.f = pF->p;
+   const bool planar = !(pF->stride[0] | pF->stride[1] | pF->stride[2]);
+   a.sx = planar ? 1 : pF->stride[0];
+   a.sy = planar ? (int64_t)X : pF->stride[1];
+   a.sz = planar ? (int64_t)X * Y : pF->stride[2];
+   a.X = X; a.Y = Y; a.Z = Z;
+   a.K = K;
+   a.out = pBPFD;
+   uint32_t masks[2];
+   for (int k = 0; k < K; k++) {
+      const double t = pT->t[k];
+      if (pF->enc == ENC_F32) { floatBoundsPlain(t, a.tlo[k], a.thi[k]); }
+      else { a.tlo[k] = a.thi[k] = t; }
+      a.outRow[k] = k;
+      masks[k] = (pT->m ? pT->m[k] : pT->mAll) & BMC_AL;
+   }
+   return launchWordsMoments(a, pF->enc, masks, pMom, s);
+}
+
 // ---------------------------------------------------------------- batches
 
 struct MKFBatchPlan

@@ -67,6 +67,7 @@ struct WordTask
    int complement;        // the map is counted negated: code c is stored in bin 255 - c
    int variant;           // batched kernel: which instantiation counts this field
    uint64_t *out;
+   double *mom;           // moments kernel: [K][2 map values][sum f, sum f^2]
    int nChunkX, nTileY, nSlabZ;
    long long nItems;
 };
@@ -118,6 +119,10 @@ int launchWordsBatch(const WordBatchArgs &b, int enc, cudaStream_t s);
 // one relation (words.cu); `masks` are the relation masks of f's (sorted) thresholds.
 // MKF_ERR_UNSUPPORTED otherwise.
 int launchWords(const FusedArgs &f, int enc, const uint32_t *masks, cudaStream_t s);
+
+// Counts and descriptive moments of one or two thresholds (any relations) in one read (words.cu):
+// mom is device double[K][2][2], per threshold and map value the sum of f and of f^2.
+int launchWordsMoments(const FusedArgs &f, int enc, const uint32_t *masks, double *mom, cudaStream_t s);
 
 // Launch the thermometer kernel for a pass whose thresholds all share one relation
 // (< <= > >=); fills the key table of `a` first.

@@ -118,11 +118,42 @@ __device__ __forceinline__ void countPlane(const T (&v)[32], WordCarry<KMAX> &c,
    }
 }
 
+// Descriptive moments of the field by map value (the original's categorical CUDAImgMom,
+// binMapCUDA.cuh:67-128): per threshold, the sum of f and of f^2 over the elements mapping to 0
+// and to 1, in FP64. Every element is added once: an item owns the elements of its cells, and the
+// items at the field's +x / +y / +z ends also the field's last column / row / plane.
+template <int KMAX>
+struct MomAcc
+{
+   double s[KMAX][2][2];
+};
+
+template <typename T, int KMAX>
+__device__ __forceinline__ void addMoments(const T (&v)[32], MomAcc<KMAX> &acc, const uint32_t *m, const T *tlo,
+                                           const T *thi, bool ownXZ, int y0, int ys, int ye, bool lastY, int Y)
+{
+#pragma unroll
+   for (int r = 0; r < 32; r++) {
+      const int y = y0 + r;
+      const bool own = ownXZ && y < Y && ((y >= ys && y < ye) || (lastY && y == Y - 1));
+      if (own) {
+         const double d = (double)v[r];
+         const double d2 = d * d;
+#pragma unroll
+         for (int k = 0; k < KMAX; k++) {
+            const uint32_t b = mapBit<T>(v[r], kGEN, m[k], tlo[k], thi[k]);
+            acc.s[k][b][0] += d;
+            acc.s[k][b][1] += d2;
+         }
+      }
+   }
+}
+
 // One warp counts work item `it` (31 x 31 cells, D planes) of field `a` into the CTA's histogram
 // and all-zeros / all-ones totals. INNER: the field is at least 32 x 32 in x and y with a positive
 // row stride below 2^32 / 31 bytes; edge tiles are then shifted back inside the field (their cells
 // already counted by the neighbouring tile are masked out), so no load needs clamping.
-template <typename T, int KMAX, int CLS0, int CLS1, bool INNER>
+template <typename T, int KMAX, int CLS0, int CLS1, bool INNER, bool MOM = false>
 __device__ __forceinline__ void wordItem(const WordTask &a, long long it, const T *tlo, const T *thi,
                                          uint32_t (*sRow)[32], uint32_t *sHist, unsigned long long (*sEnds)[2])
 {
@@ -150,10 +181,35 @@ __device__ __forceinline__ void wordItem(const WordTask &a, long long it, const 
    WordCarry<KMAX> c;
 #pragma unroll
    for (int k = 0; k < KMAX; k++) { c.n0[k] = c.n1[k] = 0; c.pw[k] = c.pn[k] = 0; }
+   MomAcc<MOM ? KMAX : 1> acc;
+   bool ownX = false, lastY = false, lastZ = false;
+   if (MOM) {
+      for (int k = 0; k < (MOM ? KMAX : 1); k++) { acc.s[k][0][0] = acc.s[k][0][1] = acc.s[k][1][0] = acc.s[k][1][1] = 0.0; }
+      const int x = x0 + lane;
+      ownX = x < a.X && ((x >= xs && x < xe) || (ix == a.nChunkX - 1 && x == a.X - 1));
+      lastY = iy == a.nTileY - 1;
+      lastZ = iz == a.nSlabZ - 1;
+   }
    for (int p = 0; p <= nPln; ++p) {
       T v[32];
       loadPlane<T, INNER>(v, base + (long long)p * a.sz, a.sy, syb, nRow);
+      if (MOM) {
+         const bool ownZ = p < nPln || (lastZ && z0 + p == a.Z - 1);
+         addMoments<T, MOM ? KMAX : 1>(v, acc, a.m, tlo, thi, ownX && ownZ, y0, ys, ye, lastY, a.Y);
+      }
       countPlane<T, KMAX, CLS0, CLS1>(v, c, a.m, tlo, thi, xin, lane, vm, p == 0, sRow, sHist);
+   }
+   if (MOM) {
+#pragma unroll
+      for (int k = 0; k < (MOM ? KMAX : 1); k++) {
+#pragma unroll
+         for (int q = 0; q < 4; q++) {
+            double x = acc.s[k][q >> 1][q & 1];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) { x += __shfl_xor_sync(FULL, x, o); }
+            if (lane == 0 && x != 0.0) { atomicAdd(a.mom + k * 4 + q, x); }
+         }
+      }
    }
 #pragma unroll
    for (int k = 0; k < KMAX; k++) {
@@ -187,7 +243,7 @@ __device__ void flushWords(const WordTask &a, uint32_t *sHist, unsigned long lon
 }
 
 // One launch counts K = KMAX thresholds of classes CLS0 (and CLS1), compile-time constants.
-template <typename T, int KMAX, int CLS0, int CLS1, bool INNER, int MINB>
+template <typename T, int KMAX, int CLS0, int CLS1, bool INNER, int MINB, bool MOM = false>
 __global__ void __launch_bounds__(kWdWarps * 32, MINB) wordBPFD(const __grid_constant__ WordTask a)
 {
    __shared__ uint32_t sHist[KMAX * 256];
@@ -208,7 +264,7 @@ __global__ void __launch_bounds__(kWdWarps * 32, MINB) wordBPFD(const __grid_con
    uint32_t (*sRow)[32] = sRows[threadIdx.x >> 5];
 
    for (long long it = gw; it < a.nItems; it += nw) {
-      wordItem<T, KMAX, CLS0, CLS1, INNER>(a, it, tlo, thi, sRow, sHist, sEnds);
+      wordItem<T, KMAX, CLS0, CLS1, INNER, MOM>(a, it, tlo, thi, sRow, sHist, sEnds);
    }
    __syncthreads();
    flushWords<KMAX>(a, sHist, sEnds);
@@ -316,6 +372,57 @@ int launchWords(const FusedArgs &f, int enc, const uint32_t *masks, cudaStream_t
    a.nItems = (long long)a.nChunkX * a.nTileY * a.nSlabZ;
    if (enc == ENC_F32) { return dispatchWords<float>(a, s); }
    return dispatchWords<double>(a, s);
+}
+
+// ---------------------------------------------------------------- counts and moments in one read
+
+template <typename T, int KMAX, bool INNER>
+static int launchMomentsI(const WordTask &a, cudaStream_t s)
+{
+   static std::atomic<int> occ{0};
+   auto kern = wordBPFD<T, KMAX, kGEN, kGEN, INNER, 2, true>;
+   const int blocksPerSM = cachedOccupancy(occ, kern, kWdWarps * 32, 0);
+   long long grid = (a.nItems + kWdWarps - 1) / kWdWarps;
+   const long long cap = (long long)smCount() * blocksPerSM;
+   if (grid > cap) { grid = cap; }
+   if (grid < 1) { grid = 1; }
+   kern<<<(unsigned)grid, kWdWarps * 32, 0, s>>>(a);
+   return cudaFail(cudaGetLastError(), "wordBPFD (moments) launch");
+}
+
+template <typename T>
+static int dispatchMoments(const WordTask &a, bool inner, cudaStream_t s)
+{
+   if (a.K == 1) { return inner ? launchMomentsI<T, 1, true>(a, s) : launchMomentsI<T, 1, false>(a, s); }
+   return inner ? launchMomentsI<T, 2, true>(a, s) : launchMomentsI<T, 2, false>(a, s);
+}
+
+int launchWordsMoments(const FusedArgs &f, int enc, const uint32_t *masks, double *mom, cudaStream_t s)
+{
+   if (f.K < 1 || f.K > 2 || f.X < 2 || f.Y < 2 || f.Z < 2) { return MKF_ERR_UNSUPPORTED; }
+   WordTask a;
+   memset(&a, 0, sizeof(a));
+   a.f = f.f;
+   a.sx = f.sx; a.sy = f.sy; a.sz = f.sz;
+   a.X = f.X; a.Y = f.Y; a.Z = f.Z;
+   a.K = f.K;
+   a.out = f.out;
+   a.mom = mom;
+   for (int k = 0; k < f.K; k++) {
+      a.m[k] = masks[k] & BMC_AL;
+      a.cls[k] = kGEN;
+      a.tlo[k] = f.tlo[k];
+      a.thi[k] = f.thi[k];
+      a.outRow[k] = f.outRow[k];
+   }
+   a.nChunkX = (a.X - 1 + 30) / 31;
+   a.nTileY = (a.Y - 1 + 30) / 31;
+   a.nSlabZ = (a.Z - 1 + kWdD - 1) / kWdD;
+   a.nItems = (long long)a.nChunkX * a.nTileY * a.nSlabZ;
+   const int64_t syb = a.sy * (enc == ENC_F32 ? 4 : 8);
+   const bool inner = a.X >= 32 && a.Y >= 32 && syb > 0 && syb * 31 < ((int64_t)1 << 32);
+   if (enc == ENC_F32) { return dispatchMoments<float>(a, inner, s); }
+   return dispatchMoments<double>(a, inner, s);
 }
 
 // ---------------------------------------------------------------- many fields, one launch

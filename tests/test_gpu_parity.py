@@ -453,3 +453,29 @@ def test_three_to_six_thresholds_of_one_relation(mkf, oracle, cuda, dtype):
             for m in (mkf.BMC_GT, mkf.BMC_GT | mkf.BMC_EQ, mkf.BMC_LT, mkf.BMC_LT | mkf.BMC_EQ):
                 got = u64(mkf.field_bpfd(to_dev(f, cuda), t, m))
                 assert (got == oracle.bpfd_field(f, (X, Y, Z), t, m)).all(), (shape, K, m)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_counts_with_moments(mkf, cuda, dtype):
+    """mkfFieldBPFDMoments: the counts equal mkfFieldBPFD's exactly; per threshold and map value
+    the sums of f and f^2 equal FP64 sums over the elements (every element once, tiles overlap),
+    within 1e-9 of the sum of magnitudes (the summation order differs)."""
+    import torch
+
+    rng = np.random.default_rng(31)
+    big = to_dev(rng.standard_normal((12, 80, 150)).astype(dtype), cuda)
+    cases = [rng.standard_normal(s).astype(dtype) for s in [(5, 6, 7), (3, 40, 33), (9, 64, 64), (35, 33, 97)]]
+    views = [to_dev(c, cuda) for c in cases] + [big[1:11, 3:70, 5:140], big[:, :, ::2]]
+    for v in views:
+        f = v.cpu().numpy().astype(np.float64)
+        for t, m in (([0.1], [4]), ([-0.3, 0.4], [6, 1]), ([0.2, 0.2], [2, 5]), ([0.0], [7])):
+            counts, mom = mkf.field_bpfd_moments(v, t, m)
+            assert (u64(counts) == u64(mkf.field_bpfd(v, t, m))).all()
+            mom = mom.cpu().numpy()
+            for k, (tk, mk) in enumerate(zip(t, m)):
+                d = 1 - (f < tk).astype(int) + (f > tk).astype(int)
+                bit = (mk >> d) & 1
+                for b in (0, 1):
+                    sel = f[bit == b]
+                    assert abs(mom[k, b, 0] - sel.sum()) <= 1e-9 * (np.abs(f).sum() + 1)
+                    assert abs(mom[k, b, 1] - (sel * sel).sum()) <= 1e-9 * ((f * f).sum() + 1)
