@@ -108,6 +108,9 @@ int mkfFieldBPFDHostNoAlloc(uint64_t *pBPFDH, const MKFFieldDesc *pF, const MKFT
  * are counted by their own pass. A plan keeps the work list on the device so the same batch (same
  * buffers, new contents) can be launched again, also inside a CUDA graph. */
 typedef struct MKFBatchPlan MKFBatchPlan;
+/* Unless mkfSetTuning(0) switched it off, creation times one launch of the batch for each candidate
+ * slab depth (planes per work item) and keeps the fastest: the fields must hold readable data, and
+ * pBPFD is written. Synchronous. */
 int mkfBatchPlanCreate(MKFBatchPlan **pPlan, uint64_t *pBPFD, const MKFFieldDesc *pF, const MKFThreshSet *pT, int nF);
 /* Clear the counts and count every field, asynchronously on `stream`; issues no allocation and no
  * synchronisation, so it may be captured into a CUDA graph. */
@@ -170,6 +173,17 @@ int mkfServerStats(MKFServer *server, MKFServerStats *stats, int reset);
  * can no longer be admitted because the budget is held by counts never released fail with
  * MKF_ERR_BUSY instead of waiting. */
 int mkfServerDestroy(MKFServer *server);
+
+/* ---- tuning (no original counterpart) ----
+ * The slab depth of a kernel (planes of cells per work item) trades halo re-reads against work
+ * items per SM. mkfTune times the candidate depths on this field with these thresholds (the
+ * counting runs several times; synchronous) and keeps the fastest for fields of the same kind:
+ * kernel, element type, threshold count and the power-of-two size class of each extent. Later
+ * mkfFieldBPFD calls on such fields use it; without tuning each kernel uses its default.
+ * mkfSetTuning(0 / 1) switches the tuning of new batch plans off / on (default on); it returns
+ * the previous setting. */
+int mkfTune(const MKFFieldDesc *pF, const MKFThreshSet *pT, void *stream);
+int mkfSetTuning(int batchPlans);
 
 /* ---- measures (closest original: mkfSelectMeasuresBPFD, mkfUtil.c:94) ---- */
 /* For each of nSets distributions (host uint64_t[nSets][256]) write, in double:

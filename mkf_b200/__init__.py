@@ -20,7 +20,7 @@ from ._lib import (BMC_AL, BMC_EQ, BMC_GT, BMC_LT, ENC_F32, ENC_F64, MKF_F_ACCUM
                    MKFServerStats, MKFThreshSet, check, lib)
 
 __all__ = [
-    "build", "lib", "MKFError", "BatchPlan", "Server", "relation_mask", "field_bpfd", "field_bpfd_moments", "field_bpfd_host", "batch_bpfd",
+    "build", "lib", "MKFError", "BatchPlan", "Server", "relation_mask", "field_bpfd", "field_bpfd_moments", "field_bpfd_host", "tune", "set_batch_tuning", "batch_bpfd",
     "bin_map_cuda", "get_bpfd", "get_bpfd_host", "measures", "measures_dev", "select_measures",
     "ENC_F32", "ENC_F64", "BMC_LT", "BMC_EQ", "BMC_GT", "BMC_AL",
 ]
@@ -125,6 +125,20 @@ def field_bpfd_moments(field, thresholds, mask=BMC_GT, stream=None):
     check(lib().mkfFieldBPFDMoments(out.data_ptr(), mom.data_ptr(), C.byref(d), C.byref(th.ts), 0, _stream_ptr(stream)),
           "mkfFieldBPFDMoments")
     return out, mom
+
+
+def tune(field, thresholds, mask=BMC_GT, stream=None) -> None:
+    """mkfTune: time the candidate slab depths on this CUDA field and keep the fastest for fields
+    of the same kind (synchronous; the counts of later calls do not change, only their speed)."""
+    th = _Thresholds(thresholds, mask)
+    strides = None if field.is_contiguous() else field.stride()
+    d = _field_desc(field.data_ptr(), _enc_of(field), field.shape, strides)
+    check(lib().mkfTune(C.byref(d), C.byref(th.ts), _stream_ptr(stream)), "mkfTune")
+
+
+def set_batch_tuning(on: bool) -> bool:
+    """Switch the tuning of new batch plans on or off; returns the previous setting."""
+    return bool(lib().mkfSetTuning(int(bool(on))))
 
 
 def field_bpfd_host(field: np.ndarray, thresholds, mask=BMC_GT) -> np.ndarray:

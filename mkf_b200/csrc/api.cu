@@ -172,9 +172,9 @@ static void freePlan(MKFBatchPlan *p)
    delete p;
 }
 
-MKF_API int mkfBatchPlanCreate(MKFBatchPlan **pp, uint64_t *pBPFD, const MKFFieldDesc *pF, const MKFThreshSet *pT, int nF)
+// A plan whose work items span `depth` planes (0: each kernel's default).
+static int createPlan(MKFBatchPlan **pp, uint64_t *pBPFD, const MKFFieldDesc *pF, const MKFThreshSet *pT, int nF, int depth)
 {
-   if (!pp || !pBPFD || (nF > 0 && (!pF || !pT)) || nF < 0) { setError("mkfBatchPlanCreate: bad argument"); return MKF_ERR_ARG; }
    *pp = nullptr;
    MKFBatchPlan *p = new MKFBatchPlan();
    p->out = pBPFD;
@@ -197,7 +197,7 @@ MKF_API int mkfBatchPlanCreate(MKFBatchPlan **pp, uint64_t *pBPFD, const MKFFiel
       FieldTask t;
       WordTask w;
       bool varying = false;
-      const int kind = planBatchField(d, ts, (int)row, t, w, p->consts, varying);
+      const int kind = planBatchField(d, ts, (int)row, t, w, p->consts, varying, depth);
       for (size_t c = c0; c < p->consts.size(); c++) { p->constCells.push_back(cells); }
       if (cells > 0 && kind == kPlanWords) {
          const int e = d->enc == ENC_F32 ? 0 : 1;
@@ -298,6 +298,52 @@ static int planLaunchOn(MKFBatchPlan *p, cudaStream_t s)
       rc = fieldBPFD(p->out + fb.rowBase * 256, &fb.d, &ts, MKF_F_ACCUMULATE, s, nullptr);
    }
    return rc;
+}
+
+MKF_API int mkfBatchPlanCreate(MKFBatchPlan **pp, uint64_t *pBPFD, const MKFFieldDesc *pF, const MKFThreshSet *pT, int nF)
+{
+   if (!pp || !pBPFD || (nF > 0 && (!pF || !pT)) || nF < 0) { setError("mkfBatchPlanCreate: bad argument"); return MKF_ERR_ARG; }
+   *pp = nullptr;
+   if (!batchTuning() || nF == 0) { return createPlan(pp, pBPFD, pF, pT, nF, 0); }
+   // time one launch of the plan for each candidate slab depth and keep the fastest
+   static const int kCand[] = {8, 16, 32, 64};
+   cudaStream_t s = nullptr;
+   cudaEvent_t e0 = nullptr, e1 = nullptr;
+   cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+   if (e == cudaSuccess) { e = cudaEventCreate(&e0); }
+   if (e == cudaSuccess) { e = cudaEventCreate(&e1); }
+   int rc = (e == cudaSuccess) ? MKF_OK : cudaFail(e, "mkfBatchPlanCreate: tuning set-up");
+   MKFBatchPlan *best = nullptr;
+   float bestMs = 0.0f;
+   for (int c = 0; c < 4 && rc == MKF_OK; c++) {
+      MKFBatchPlan *cand = nullptr;
+      rc = createPlan(&cand, pBPFD, pF, pT, nF, kCand[c]);
+      if (rc != MKF_OK) { break; }
+      rc = planLaunchOn(cand, s);  // warm-up
+      if (rc == MKF_OK && (e = cudaEventRecord(e0, s)) != cudaSuccess) { rc = cudaFail(e, "event"); }
+      if (rc == MKF_OK) { rc = planLaunchOn(cand, s); }
+      if (rc == MKF_OK && (e = cudaEventRecord(e1, s)) != cudaSuccess) { rc = cudaFail(e, "event"); }
+      if (rc == MKF_OK && (e = cudaEventSynchronize(e1)) != cudaSuccess) { rc = cudaFail(e, "event"); }
+      float ms = 0.0f;
+      if (rc == MKF_OK && (e = cudaEventElapsedTime(&ms, e0, e1)) != cudaSuccess) { rc = cudaFail(e, "event"); }
+      if (rc == MKF_OK && (!best || ms < bestMs)) {
+         if (best) { freePlan(best); }
+         best = cand;
+         bestMs = ms;
+      } else {
+         cudaStreamSynchronize(s);
+         freePlan(cand);
+      }
+   }
+   if (s) { cudaStreamSynchronize(s); cudaStreamDestroy(s); }
+   if (e0) { cudaEventDestroy(e0); }
+   if (e1) { cudaEventDestroy(e1); }
+   if (rc != MKF_OK) {
+      if (best) { freePlan(best); }
+      return rc;
+   }
+   *pp = best;
+   return MKF_OK;
 }
 
 MKF_API int mkfBatchPlanLaunch(MKFBatchPlan *p, void *stream)

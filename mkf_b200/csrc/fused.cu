@@ -334,7 +334,7 @@ void floatBoundsPlain(double t, double &tlo, double &thi) { floatBounds(t, tlo, 
 // share one thermometer relation and fit the rank table fill `t` for the batched thermometer
 // kernel (kPlanThermo); otherwise the field takes the single-field path (kPlanSingle).
 int planBatchField(const MKFFieldDesc *pF, const MKFThreshSet *pT, int rowBase, FieldTask &t, WordTask &w,
-                   std::vector<ConstEntry> &consts, bool &anyVarying)
+                   std::vector<ConstEntry> &consts, bool &anyVarying, int depth)
 {
    memset(&t, 0, sizeof(t));
    memset(&w, 0, sizeof(w));
@@ -375,7 +375,7 @@ int planBatchField(const MKFFieldDesc *pF, const MKFThreshSet *pT, int rowBase, 
          w.m[k] = (pT->m ? pT->m[idx[k]] : pT->mAll) & BMC_AL;
          w.outRow[k] = rowBase + idx[k];
       }
-      prepareWordTask(w, pF->enc);
+      prepareWordTask(w, pF->enc, depth);
       return kPlanWords;
    }
    if (cls0 < 0) { return kPlanSingle; }
@@ -397,7 +397,7 @@ int planBatchField(const MKFFieldDesc *pF, const MKFThreshSet *pT, int rowBase, 
    t.complement = (cls0 >= 2);
    const bool eqBit = (cls0 == 1 || cls0 == 3);
    t.nanRank = (eqBit != (t.complement != 0)) ? (uint32_t)n : 0u;
-   return prepareThermoTask(t, pF->enc) ? kPlanThermo : kPlanSingle;
+   return prepareThermoTask(t, pF->enc, depth) ? kPlanThermo : kPlanSingle;
 }
 
 int fieldBPFD(uint64_t *out, const MKFFieldDesc *pF, const MKFThreshSet *pT, int flags, cudaStream_t s,

@@ -68,6 +68,7 @@ struct WordTask
    int variant;           // batched kernel: which instantiation counts this field
    uint64_t *out;
    double *mom;           // moments kernel: [K][2 map values][sum f, sum f^2]
+   int D, pad_;           // planes of cells per work item
    int nChunkX, nTileY, nSlabZ;
    long long nItems;
 };
@@ -102,17 +103,24 @@ int fieldBPFD(uint64_t *out, const MKFFieldDesc *pF, const MKFThreshSet *pT, int
 
 enum { kPlanSingle = 0, kPlanThermo = 1, kPlanWords = 2 };
 int planBatchField(const MKFFieldDesc *pF, const MKFThreshSet *pT, int rowBase, FieldTask &t, WordTask &w,
-                   std::vector<ConstEntry> &consts, bool &anyVarying);
+                   std::vector<ConstEntry> &consts, bool &anyVarying, int depth = 0);
+
+// Slab depth (planes of cells per work item) of a single-field launch of kernel family `family`
+// (tune.cu): the depth mkfTune measured best for this kind of field, else `def`.
+enum { kFamWords = 0, kFamThermo = 1 };
+int tunedDepth(int family, int enc, int K, int X, int Y, int Z, int def);
+// Whether mkfBatchPlanCreate measures the slab depth of each new plan (tune.cu).
+bool batchTuning();
 
 // Fill a task's key table and item grid; false if its thresholds share a rank-table bucket.
-bool prepareThermoTask(FieldTask &t, int enc);
+bool prepareThermoTask(FieldTask &t, int enc, int depth = 0);
 // Launch the batched thermometer kernel over tasks of one element type (enc) whose largest
 // threshold count is maxK.
 int launchThermoBatch(const BatchArgs &b, int enc, int maxK, cudaStream_t s);
 
 // Fill a word task's relation classes, batched variant and item grid (words.cu); launch the
 // batched word kernel over the chunks of tasks of one element type.
-void prepareWordTask(WordTask &a, int enc);
+void prepareWordTask(WordTask &a, int enc, int depth = 0);
 int launchWordsBatch(const WordBatchArgs &b, int enc, cudaStream_t s);
 
 // Word-parallel kernel for one or two thresholds of any relations, or up to kWordMaxK thresholds of

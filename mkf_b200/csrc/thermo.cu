@@ -33,6 +33,9 @@ static constexpr int kThWarps = 8;
 #ifndef THERMO_MINB
 #define THERMO_MINB (THERMO_TY == 8 ? 3 : 2)
 #endif
+#ifndef THERMO_D
+#define THERMO_D 64  // default planes of cells per work item
+#endif
 #ifndef THERMO_BATCH_MINB
 #define THERMO_BATCH_MINB 2  // the per-field variant switch needs the larger register budget
 #endif
@@ -559,12 +562,12 @@ static void itemGrid(P &a, int D)
    a.nItems = (long long)a.nSegX * a.nTileY * a.nSlabZ;
 }
 
-bool prepareThermoTask(FieldTask &t, int enc)
+bool prepareThermoTask(FieldTask &t, int enc, int depth)
 {
    t.lutC = prepareKeys(t, enc);
    if (t.lutC == 0) { return false; }
    t.variant = (enc == ENC_F32 ? 0 : 2) + (t.rankHi ? 1 : 0) + (innerTiles(t, enc) ? 4 : 0) + (t.lutC > 1 ? 8 : 0);
-   itemGrid(t, 32);
+   itemGrid(t, depth > 0 ? depth : THERMO_D);
    return true;
 }
 
@@ -600,7 +603,7 @@ int launchThermo(FusedArgs &a, int enc, cudaStream_t s)
 {
    a.lutC = prepareKeys(a, enc);
    if (a.lutC == 0) { return MKF_ERR_UNSUPPORTED; }
-   itemGrid(a, 32);
+   itemGrid(a, tunedDepth(kFamThermo, enc, a.K, a.X, a.Y, a.Z, THERMO_D));
    const bool ge = a.rankHi != 0, inner = innerTiles(a, enc);
    if (enc == ENC_F32) { return ge ? launchThermoG<float, true>(a, inner, s) : launchThermoG<float, false>(a, inner, s); }
    return ge ? launchThermoG<double, true>(a, inner, s) : launchThermoG<double, false>(a, inner, s);

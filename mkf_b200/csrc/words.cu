@@ -1,4 +1,5 @@
-// words.cu - fused counting kernel for one or two thresholds (any relations), word-parallel.
+// words.cu - fused counting kernel for one or two thresholds of any relations, or up to six of one
+// relation, word-parallel (optionally with the field's moments per map value from the same read).
 //
 // With few thresholds the per-element cost must be a handful of instructions, so cells are
 // handled 32 at a time as bit words, as the original's packed binary map does
@@ -22,7 +23,10 @@ namespace mkf {
 #endif
 
 static constexpr int kWdWarps = 8;
-static constexpr int kWdD = 32;
+#ifndef WORDS_D
+#define WORDS_D 32
+#endif
+static constexpr int kWdD = WORDS_D;  // default planes of cells per work item (WordTask::D)
 
 // Relation class of a threshold: every class is one comparison (NaN maps as the EQ bit says).
 enum WordCls { kGT = 0, kGE = 1, kLT = 2, kLE = 3, kGEN = 4 };
@@ -165,9 +169,9 @@ __device__ __forceinline__ void wordItem(const WordTask &a, long long it, const 
    const int iy = (int)(rest % a.nTileY);
    const int iz = (int)(rest / a.nTileY);
    // this item's cells: x in [xs, xe), y in [ys, ye), z in [z0, z0 + nPln)
-   const int xs = 31 * ix, ys = 31 * iy, z0 = kWdD * iz;
+   const int xs = 31 * ix, ys = 31 * iy, z0 = a.D * iz;
    const int xe = min(xs + 31, a.X - 1), ye = min(ys + 31, a.Y - 1);
-   const int nPln = min(kWdD, a.Z - 1 - z0);
+   const int nPln = min(a.D, a.Z - 1 - z0);
    // tile origin: bit b of a word is x0 + b, lane l counts the row pair y0 + l
    const int x0 = INNER ? min(xs, a.X - 32) : xs;
    const int y0 = INNER ? min(ys, a.Y - 32) : ys;
@@ -368,7 +372,8 @@ int launchWords(const FusedArgs &f, int enc, const uint32_t *masks, cudaStream_t
    }
    a.nChunkX = (a.X - 1 + 30) / 31;
    a.nTileY = (a.Y - 1 + 30) / 31;
-   a.nSlabZ = (a.Z - 1 + kWdD - 1) / kWdD;
+   a.D = tunedDepth(kFamWords, enc, a.K, a.X, a.Y, a.Z, kWdD);
+   a.nSlabZ = (a.Z - 1 + a.D - 1) / a.D;
    a.nItems = (long long)a.nChunkX * a.nTileY * a.nSlabZ;
    if (enc == ENC_F32) { return dispatchWords<float>(a, s); }
    return dispatchWords<double>(a, s);
@@ -417,7 +422,8 @@ int launchWordsMoments(const FusedArgs &f, int enc, const uint32_t *masks, doubl
    }
    a.nChunkX = (a.X - 1 + 30) / 31;
    a.nTileY = (a.Y - 1 + 30) / 31;
-   a.nSlabZ = (a.Z - 1 + kWdD - 1) / kWdD;
+   a.D = kWdD;
+   a.nSlabZ = (a.Z - 1 + a.D - 1) / a.D;
    a.nItems = (long long)a.nChunkX * a.nTileY * a.nSlabZ;
    const int64_t syb = a.sy * (enc == ENC_F32 ? 4 : 8);
    const bool inner = a.X >= 32 && a.Y >= 32 && syb > 0 && syb * 31 < ((int64_t)1 << 32);
@@ -488,7 +494,7 @@ __global__ void __launch_bounds__(kWdWarps * 32, MINB) wordBatch(const __grid_co
 
 // Fill a word task from a field with one or two varying thresholds (sorted rows and bounds in
 // `f`, relation masks in `masks`): relation classes, the batched variant and the item grid.
-void prepareWordTask(WordTask &a, int enc)
+void prepareWordTask(WordTask &a, int enc, int depth)
 {
    int kind;
    for (int k = 0; k < a.K; k++) {
@@ -512,7 +518,8 @@ void prepareWordTask(WordTask &a, int enc)
    a.variant = kind + (inner ? 4 : 0);
    a.nChunkX = (a.X - 1 + 30) / 31;
    a.nTileY = (a.Y - 1 + 30) / 31;
-   a.nSlabZ = (a.Z - 1 + kWdD - 1) / kWdD;
+   a.D = depth > 0 ? depth : kWdD;
+   a.nSlabZ = (a.Z - 1 + a.D - 1) / a.D;
    a.nItems = (long long)a.nChunkX * a.nTileY * a.nSlabZ;
 }
 

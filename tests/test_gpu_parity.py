@@ -479,3 +479,35 @@ def test_counts_with_moments(mkf, cuda, dtype):
                     sel = f[bit == b]
                     assert abs(mom[k, b, 0] - sel.sum()) <= 1e-9 * (np.abs(f).sum() + 1)
                     assert abs(mom[k, b, 1] - (sel * sel).sum()) <= 1e-9 * ((f * f).sum() + 1)
+
+
+def test_tuning_keeps_counts(mkf, cuda):
+    """Slab-depth tuning changes speed only: counts before and after mkfTune, and of batch plans
+    created with and without tuning, are identical."""
+    import torch
+
+    g = torch.Generator(device=cuda).manual_seed(8)
+    f64 = torch.randn((150, 200, 300), dtype=torch.float64, device=cuda, generator=g)
+    f32 = torch.randn((70, 90, 130), dtype=torch.float32, device=cuda, generator=g)
+    cases = [(f64, np.linspace(-1.5, 1.5, 16)), (f32, [0.2]), (f32, [-0.5, 0.0, 0.5])]
+    before = [u64(mkf.field_bpfd(f, t, 4)) for f, t in cases]
+    for f, t in cases:
+        mkf.tune(f, t, 4)
+    for (f, t), b in zip(cases, before):
+        assert (u64(mkf.field_bpfd(f, t, 4)) == b).all()
+    fields = [f64, f32, f32[:40, :50, :60]]
+    ths = [np.linspace(-1.5, 1.5, 16), [0.2], [0.1, 0.3]]
+    plans = []
+    prev = mkf.set_batch_tuning(False)
+    try:
+        plans.append(mkf.BatchPlan(fields, ths))
+        mkf.set_batch_tuning(True)
+        plans.append(mkf.BatchPlan(fields, ths))
+    finally:
+        mkf.set_batch_tuning(prev)
+    a = u64(plans[0].launch())
+    b = u64(plans[1].launch())
+    assert (a == b).all()
+    assert (a[:16] == before[0]).all()
+    for p in plans:
+        p.close()
