@@ -383,8 +383,10 @@ MKF_API int mkfBatchPlanDestroy(MKFBatchPlan *p)
 MKF_API int mkfBatchBPFD(uint64_t *pBPFD, const MKFFieldDesc *pF, const MKFThreshSet *pT, int nF, int flags, void *stream)
 {
    (void)flags;
+   if (!pBPFD || (nF > 0 && (!pF || !pT)) || nF < 0) { setError("mkfBatchBPFD: bad argument"); return MKF_ERR_ARG; }
    MKFBatchPlan *p = nullptr;
-   int rc = mkfBatchPlanCreate(&p, pBPFD, pF, pT, nF);
+   // one launch: no depth tuning (it would count the batch several times), depth by field size
+   int rc = createPlan(&p, pBPFD, pF, pT, nF, -1);
    if (rc != MKF_OK) { return rc; }
    rc = planLaunchOn(p, (cudaStream_t)stream);
    const cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);

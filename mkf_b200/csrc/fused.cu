@@ -338,6 +338,12 @@ int planBatchField(const MKFFieldDesc *pF, const MKFThreshSet *pT, int rowBase, 
 {
    memset(&t, 0, sizeof(t));
    memset(&w, 0, sizeof(w));
+   if (depth < 0) {
+      // by size: shallow work items for small fields, so that a launch over many of them has
+      // items enough for every SM (measured best for batches of fields up to ~400^3)
+      const double vox = (double)pF->def[0] * (double)pF->def[1] * (double)pF->def[2];
+      depth = vox <= (double)(1 << 25) ? 8 : 0;
+   }
    const int K = pT->nT;
    int idx[MKF_MAX_THRESH], n = 0, cls0 = -2;
    for (int i = 0; i < K; i++) {

@@ -102,6 +102,7 @@ struct ConstEntry { int row, bin; };
 int fieldBPFD(uint64_t *out, const MKFFieldDesc *pF, const MKFThreshSet *pT, int flags, cudaStream_t s, const int *rowBase);
 
 enum { kPlanSingle = 0, kPlanThermo = 1, kPlanWords = 2 };
+// depth: planes of cells per work item; 0 = each kernel's default, -1 = chosen by field size.
 int planBatchField(const MKFFieldDesc *pF, const MKFThreshSet *pT, int rowBase, FieldTask &t, WordTask &w,
                    std::vector<ConstEntry> &consts, bool &anyVarying, int depth = 0);
 

@@ -242,7 +242,7 @@ static int issueLaunch(MKFServer *s, LaunchSlot &sl)
       WordTask w;
       std::vector<ConstEntry> ce;
       bool varying = false;
-      const int kind = planBatchField(&d, &ts, 0, t, w, ce, varying);
+      const int kind = planBatchField(&d, &ts, 0, t, w, ce, varying, -1);  // depth by field size
       if (cells == 0) { continue; }
       if (kind == kPlanSingle && varying) {
          singles.push_back({r, d});  // counts every threshold, constant maps included
