@@ -519,11 +519,16 @@ def reference_sample(f: np.ndarray, planes: int, threads: int):
 
 
 def calibrate_planes(f: np.ndarray, threads: int, target_s: float, max_planes: int) -> int:
-    """Plane pairs per sample for about target_s seconds of reference work (timed on 8 planes, so
-    that thread start-up is a small part of the measurement)."""
-    n = min(8, max_planes)
-    dt, _, _, _ = reference_sample(f, n, threads)
-    return int(max(2, min(max_planes, n * target_s / max(dt, 1e-4))))
+    """Plane pairs per sample for about target_s seconds of reference work: a two-point fit (8 and
+    32 planes) separates the per-plane cost from the fixed cost of each call's thread start-up."""
+    n1, n2 = min(8, max_planes), min(32, max_planes)
+    t1, _, _, _ = reference_sample(f, n1, threads)
+    if n2 <= n1:
+        return int(max(2, min(max_planes, n1 * target_s / max(t1, 1e-4))))
+    t2, _, _, _ = reference_sample(f, n2, threads)
+    per_plane = max((t2 - t1) / (n2 - n1), 1e-6)
+    fixed = max(t1 - n1 * per_plane, 0.0)
+    return int(max(2, min(max_planes, (target_s - fixed) / per_plane)))
 
 
 def cpu_baseline(f: np.ndarray, target_s: float = 10.0):
