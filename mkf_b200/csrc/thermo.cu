@@ -39,7 +39,8 @@ static constexpr int kThWarps = 8;
 #ifndef THERMO_BATCH_MINB
 #define THERMO_BATCH_MINB 2  // the per-field variant switch needs the larger register budget
 #endif
-static constexpr int kThSlots = 3;  // predicated mixed-code slots per cell (K > 1)
+static constexpr int kThSlots = 3;
+static constexpr int kThMaxDepth = 255;  // planes per work item the all-ones counters can hold  // predicated mixed-code slots per cell (K > 1)
 static constexpr int kLutShift = 18;
 static constexpr int kLutSize = 1 << (32 - kLutShift);
 
@@ -91,7 +92,9 @@ struct PlaneOnes
 {
    static_assert(NROW == 8 || NROW == 16, "tree of 8 or 16 rows");
    uint32_t ones = 0, twos = 0, fours = 0, eights = 0;
-   uint32_t hi[6] = {0, 0, 0, 0, 0, 0};  // counts of NROW-weight carries (up to 63 per item)
+   // bit-sliced counts of the NROW-weight carries: at most one carry per plane, so an item of up
+   // to kThMaxDepth planes needs 8 slices (a 6-slice count wraps at 64 planes of all-ones cells)
+   uint32_t hi[8] = {0, 0, 0, 0, 0, 0, 0, 0};
    uint32_t p1 = 0, p2 = 0, p4 = 0, p8 = 0;
    __device__ __forceinline__ static void fa(uint32_t &s, uint32_t &c, uint32_t a, uint32_t b, uint32_t d)
    {
@@ -101,7 +104,7 @@ struct PlaneOnes
    __device__ __forceinline__ void ripple(uint32_t c)
    {
 #pragma unroll
-      for (int i = 0; i < 6; i++) {
+      for (int i = 0; i < 8; i++) {
          const uint32_t t = hi[i] & c;
          hi[i] ^= c;
          c = t;
@@ -126,7 +129,7 @@ struct PlaneOnes
    {
       uint32_t v = ((ones >> k) & 1u) + 2u * ((twos >> k) & 1u) + 4u * ((fours >> k) & 1u) + 8u * ((eights >> k) & 1u);
 #pragma unroll
-      for (int i = 0; i < 6; i++) { v += ((uint32_t)NROW << i) * ((hi[i] >> k) & 1u); }
+      for (int i = 0; i < 8; i++) { v += ((uint32_t)NROW << i) * ((hi[i] >> k) & 1u); }
       return v;
    }
 };
@@ -554,6 +557,7 @@ static int prepareKeys(P &a, int enc)
 template <typename P>
 static void itemGrid(P &a, int D)
 {
+   D = D < 1 ? 1 : (D > kThMaxDepth ? kThMaxDepth : D);  // the all-ones counters hold kThMaxDepth planes
    constexpr int TY = THERMO_TY;
    a.D = D;
    a.nSegX = (a.X - 1 + 30) / 31;

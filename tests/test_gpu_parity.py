@@ -511,3 +511,55 @@ def test_tuning_keeps_counts(mkf, cuda):
     assert (a[:16] == before[0]).all()
     for p in plans:
         p.close()
+
+
+def test_batch_fields_with_three_to_six_thresholds(mkf, oracle, cuda):
+    """Batched fields with 3..6 thresholds of one relation (the rank-table batch kernel; the
+    single-field calls take the word kernel up to 5 / 6 thresholds) equal the single-field counts,
+    which equal the oracle's."""
+    rng = np.random.default_rng(44)
+    fields, ths, masks, host = [], [], [], []
+    for i in range(16):
+        dt = np.float32 if i % 2 else np.float64
+        shape = (int(rng.integers(4, 40)), int(rng.integers(20, 70)), int(rng.integers(20, 90)))
+        f = (rng.integers(-8, 9, size=shape) * 0.25).astype(dt)
+        K = 3 + i % 4
+        t = list(np.round(rng.uniform(-1.5, 1.5, size=K) * 4) / 4)
+        m = [mkf.BMC_GT, mkf.BMC_GT | mkf.BMC_EQ, mkf.BMC_LT, mkf.BMC_LT | mkf.BMC_EQ][(i // 4) % 4]
+        fields.append(to_dev(f, cuda)); ths.append(t); masks.append(m); host.append(f)
+    want = []
+    for f, fd, t, m in zip(host, fields, ths, masks):
+        Z, Y, X = f.shape
+        w = u64(mkf.field_bpfd(fd, t, m))
+        assert (w == oracle.bpfd_field(f, (X, Y, Z), t, m)).all()
+        want.append(w)
+    plan = mkf.BatchPlan(fields, ths, masks)
+    assert (u64(plan.launch()) == np.concatenate(want)).all()
+    plan.close()
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_rank_table_kernel_on_all_ones_regions(mkf, oracle, cuda, dtype):
+    """Large regions above every threshold: work items of 64 (default) and 128 (tuned) planes
+    whose columns are all-ones for every threshold, single-field and batched, against the oracle.
+    (Their all-ones counters must hold a carry per plane: 64 planes of all-ones cells once wrapped
+    a 6-slice counter.)"""
+    rng = np.random.default_rng(57)
+    fields, want, ths = [], [], []
+    for shape in [(140, 40, 70), (200, 24, 50), (70, 33, 65)]:
+        f = np.full(shape, 5.0) + rng.standard_normal(shape) * 0.01
+        Z, Y, X = shape
+        for _ in range(3):  # a few dips below the thresholds
+            z, y, x = (int(rng.integers(0, n)) for n in shape)
+            f[max(0, z - 6):z + 6, max(0, y - 6):y + 6, max(0, x - 6):x + 6] = rng.uniform(-2, 2)
+        f = f.astype(dtype)
+        t = list(np.linspace(-1.5, 1.5, 8))  # 8 thresholds of one relation: the rank-table kernel
+        w = oracle.bpfd_field(f, (X, Y, Z), t, mkf.BMC_GT)
+        fd = to_dev(f, cuda)
+        assert (u64(mkf.field_bpfd(fd, t, mkf.BMC_GT)) == w).all(), shape
+        mkf.tune(fd, t, mkf.BMC_GT)
+        assert (u64(mkf.field_bpfd(fd, t, mkf.BMC_GT)) == w).all(), shape
+        fields.append(fd); want.append(w); ths.append(t)
+    plan = mkf.BatchPlan(fields, ths)
+    assert (u64(plan.launch()) == np.concatenate(want)).all()
+    plan.close()
