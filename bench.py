@@ -627,6 +627,11 @@ def run_mkf(args, rank, world, local_rank):
     sampler.stop()
     ms = e0.elapsed_time(e1)
     kern_ms = float(np.mean([a.elapsed_time(b) for a, b in ev_k]))
+    # the timed kernel's counts against a different kernel (one threshold at a time, word-parallel)
+    # (one GPU: with several, `out` holds the all-reduced counts of every rank's slab)
+    checked = None if world > 1 else all(
+        bool(torch.equal(out[k:k + 1], mkf_b200.field_bpfd(f, THRESHOLDS[k:k + 1], mkf_b200.BMC_GT)))
+        for k in (0, K_THRESH // 2, K_THRESH - 1))
     t = torch.tensor([ms, kern_ms], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -679,6 +684,7 @@ def run_mkf(args, rank, world, local_rank):
         "roofline": roof,
         "e2e": e2e,
         "gpu_launches": 2 * args.steps,
+        "counts_checked_against_word_kernel": checked,
         "clocks": clocks,
     }
     if world == 1 and not args.no_cpu_baseline:
