@@ -1,6 +1,9 @@
 """Parity of the CUDA library (through its C ABI) with the oracle and the reference's golden
 vectors. Integer outputs must be bit-exact; the double measures must equal the host's exactly.
 Needs a B200 (`-m gpu`)."""
+import os
+import sys
+
 import numpy as np
 import pytest
 
@@ -563,3 +566,28 @@ def test_rank_table_kernel_on_all_ones_regions(mkf, oracle, cuda, dtype):
     plan = mkf.BatchPlan(fields, ths)
     assert (u64(plan.launch()) == np.concatenate(want)).all()
     plan.close()
+
+
+def test_full_size_smooth_field_two_kernels_agree(mkf, cuda):
+    """1024^3 FP64 smooth Gaussian field (sigma 4, as the benchmark's): each of the 16 rows of the
+    rank-table pass equals a single-threshold pass of the word kernel (a different algorithm), at
+    the default slab depth and at the tuned one. Smooth fields give long runs of all-ones cells,
+    which the white-noise fields of the other full-size test never do."""
+    import torch
+
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    if repo not in sys.path:
+        sys.path.insert(0, repo)
+    import bench
+
+    f = bench.grf_torch(1024, 1024, 1024, 3, cuda)
+    t = np.linspace(-2, 2, 16)
+    for tuned in (False, True):
+        if tuned:
+            mkf.tune(f, t, mkf.BMC_GT)
+        h = u64(mkf.field_bpfd(f, t, mkf.BMC_GT))
+        assert (h.sum(axis=1) == 1023 ** 3).all()
+        for k in range(16):
+            assert (u64(mkf.field_bpfd(f, t[k:k + 1], mkf.BMC_GT))[0] == h[k]).all(), (tuned, k)
+    del f
+    torch.cuda.empty_cache()
