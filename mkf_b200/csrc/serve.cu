@@ -17,71 +17,12 @@
 #include <string>
 #include <thread>
 #include <vector>
+#include "arena.h"
 #include "fused.cuh"
 
 using Clock = std::chrono::steady_clock;
 
 namespace mkf {
-
-// One device allocation of the whole budget, handed out in 256-byte-aligned blocks (best fit,
-// neighbours merged on release). Used by the worker thread only.
-class Arena
-{
- public:
-   cudaError_t init(size_t bytes)
-   {
-      size_ = bytes;
-      cudaError_t e = cudaMalloc(&base_, bytes);
-      if (e == cudaSuccess) { free_[0] = bytes; }
-      return e;
-   }
-   ~Arena()
-   {
-      if (base_) { cudaFree(base_); }
-   }
-   static size_t round(size_t n) { return (n + 255) & ~(size_t)255; }
-   void *alloc(size_t n)
-   {
-      n = round(n);
-      auto best = free_.end();
-      for (auto it = free_.begin(); it != free_.end(); ++it) {
-         if (it->second >= n && (best == free_.end() || it->second < best->second)) { best = it; }
-      }
-      if (best == free_.end()) { return nullptr; }
-      const size_t off = best->first, sz = best->second;
-      free_.erase(best);
-      if (sz > n) { free_[off + n] = sz - n; }
-      used_ += n;
-      return base_ + off;
-   }
-   void release(void *p, size_t n)
-   {
-      if (!p) { return; }
-      n = round(n);
-      size_t off = (size_t)((char *)p - base_);
-      used_ -= n;
-      auto next = free_.lower_bound(off);
-      if (next != free_.end() && off + n == next->first) {
-         n += next->second;
-         next = free_.erase(next);
-      }
-      if (next != free_.begin()) {
-         auto prev = std::prev(next);
-         if (prev->first + prev->second == off) {
-            prev->second += n;
-            return;
-         }
-      }
-      free_[off] = n;
-   }
-   size_t size() const { return size_; }
-   size_t used() const { return used_; }
-
- private:
-   char *base_ = nullptr;
-   size_t size_ = 0, used_ = 0;
-   std::map<size_t, size_t> free_;  // offset -> bytes
-};
 
 enum ReqState { kQueued, kRunning, kDone };
 
@@ -166,7 +107,8 @@ struct MKFServer
 {
    int device = 0;
    int maxPerLaunch = 256;
-   Arena arena;
+   Arena arena;          // sub-allocates `budgetMem`
+   void *budgetMem = nullptr;
    cudaStream_t copyStream = nullptr;
    LaunchSlot slots[2];
    std::mutex mu;
@@ -478,7 +420,8 @@ MKF_API int mkfServerCreate(MKFServer **ps, const MKFServerConfig *cfg)
    s->maxPerLaunch = cfg && cfg->maxFieldsPerLaunch > 0 ? cfg->maxFieldsPerLaunch : 256;
    s->device = cfg ? cfg->device : 0;
    cudaError_t e = cudaSetDevice(s->device);
-   if (e == cudaSuccess) { e = s->arena.init(budget); }
+   if (e == cudaSuccess) { e = cudaMalloc(&s->budgetMem, budget); }
+   if (e == cudaSuccess) { s->arena.init(s->budgetMem, budget); }
    if (e == cudaSuccess) { e = cudaStreamCreateWithFlags(&s->copyStream, cudaStreamNonBlocking); }
    for (LaunchSlot &sl : s->slots) {
       if (e == cudaSuccess) { e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking); }
@@ -646,6 +589,7 @@ MKF_API int mkfServerDestroy(MKFServer *s)
       sl.results.destroy();
    }
    if (s->copyStream) { cudaStreamDestroy(s->copyStream); }
+   if (s->budgetMem) { cudaFree(s->budgetMem); }
    delete s;
    return MKF_OK;
 }
