@@ -362,6 +362,8 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
          }
          continue;
       }
+      uint4 wq[TY];  // cells of this plane spanning more than 3 thresholds (about 1 in 100)
+      int nwq = 0;
 #pragma unroll
       for (int j = 0; j < TY; ++j) {
          rR = __shfl_down_sync(FULL, r[j + 1], 1);
@@ -375,10 +377,10 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
          ones.add(j, thermo(rmin) & vmask);
          {
             // Mixed codes, k = rmin .. rmax - 1. With d = corner rank - rmin per byte, the code
-            // for k = rmin + q marks the corners with d > q; with b0, b1, b2 the masks of corners
-            // whose d has bit 0, 1, 2 set, the codes for a spread rmax - rmin up to 3 are
-            // b0 | b1, b1, b0 & b1, and up to 7 (about 1 cell in 100) seven formulas in b0..b2.
-            // Wider cells count their codes one threshold at a time.
+            // for k = rmin + q marks the corners with d > q; with b0, b1 the masks of corners
+            // whose d has bit 0, 1 set, the codes for a spread rmax - rmin up to 3 are b0 | b1,
+            // b1, b0 & b1. Wider cells (about 1 in 100) are queued and count their codes one
+            // threshold at a time after the row loop.
             const uint32_t R0 = sF[j], R1 = fc;
             const uint32_t spread = rmax - rmin;
             const uint32_t rowAddr = hist32 + rmin * (kHistRow * 4);
@@ -393,23 +395,9 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
                redShared(fast && spread > 0 ? rowAddr + ((b0 | b1) << 2) : trash);
                redShared(fast && spread > 1 ? rowAddr + kHistRow * 4 + (b1 << 2) : trash);
                redShared(fast && spread > 2 ? rowAddr + kHistRow * 8 + ((b0 & b1) << 2) : trash);
-               if (!fast) {
-                  if (spread < 8) {
-                     const uint32_t b2 = gatherCode(((D0 << 1) & 0x08080808u) | ((D1 << 5) & 0x80808080u));
-                     const uint32_t c[7] = {b0 | b1 | b2, b1 | b2,      b2 | (b1 & b0), b2,
-                                            b2 & (b1 | b0), b2 & b1, b2 & b1 & b0};
-#pragma unroll
-                     for (int q = 0; q < 7; ++q) {
-                        redShared((uint32_t)q < spread ? rowAddr + q * (kHistRow * 4) + (c[q] << 2) : trash);
-                     }
-                  } else {
-                     uint32_t C = 0x7F7F7F7Fu - rb, addr = rowAddr;
-                     for (uint32_t k = rmin; k < rmax; ++k) {
-                        redShared(addr + (cellCode(R0, R1, C) << 2));
-                        C -= 0x01010101u;
-                        addr += kHistRow * 4;
-                     }
-                  }
+               if (!fast) {  // counted after the row loop: one copy of that code, not one per row
+                  wq[nwq] = make_uint4(R0, R1, rmin, rmax);
+                  ++nwq;
                }
             }
          }
@@ -418,6 +406,16 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
          ePrev = e;
          mnPrev = mn;
          mxPrev = mx;
+      }
+      // wide cells: every code k = rmin .. rmax - 1 from the packed corner ranks
+      for (int i = 0; i < nwq; ++i) {
+         const uint32_t R0 = wq[i].x, R1 = wq[i].y, rmin = wq[i].z, rmax = wq[i].w;
+         uint32_t C = 0x7F7F7F7Fu - rmin * 0x01010101u, addr = hist32 + rmin * (kHistRow * 4);
+         for (uint32_t k = rmin; k < rmax; ++k) {
+            redShared(addr + (cellCode(R0, R1, C) << 2));
+            C -= 0x01010101u;
+            addr += kHistRow * 4;
+         }
       }
    }
    for (int k = 0; k < K; ++k) {
