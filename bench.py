@@ -15,7 +15,8 @@ Inputs are 8.6 GB, far larger than the 126 MB L2, so no flush is needed between 
 
 With torchrun (N > 1) every rank counts its own 1024^3 slab (1025 planes: one halo plane) of a
 field sharded along z and the 16 x 256 partial counts are summed with an NCCL all-reduce each
-step (weak scaling). `--impl reference` times the reference C path alone (rank 0).
+step (weak scaling). `--impl reference` times the reference C path alone (rank 0) and, as a
+second reference point under "reference_cuda", the reference's own CUDA path compiled for sm_100a.
 """
 from __future__ import annotations
 
@@ -49,7 +50,7 @@ def parse():
     ap.add_argument("--impl", default="mkf", choices=["mkf", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-secondary", action="store_true", help="skip the batched and serving workloads")
+    ap.add_argument("--no-secondary", action="store_true", help="skip the batched, serving and in-situ workloads (and the reference CUDA point of the reference arm)")
     return ap.parse_args()
 
 
@@ -226,6 +227,51 @@ def serving_pool(dev, n=48, seed=SEED + 4):
         pool.append(f)
     torch.cuda.synchronize(dev)
     return pool
+
+
+def run_plain_workload(dev, steps=20, warmup=5):
+    """The plain method's workload (256^3 FP32 ball, threshold 0, '>'): the fused call
+    (mkfFieldBPFD) and the drop-in pair (binMapCUDA + mkfCUDAGetBPFD), field resident in HBM, L2
+    flushed before each call (the field is 67 MB, inside the 126 MB L2), CUDA events per call."""
+    import torch
+
+    import mkf_b200
+
+    f = ball256_torch(dev)
+    n = f.numel()
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(64 << 20, dtype=torch.int32, device=dev)
+    out = torch.zeros((1, 256), dtype=torch.int64, device=dev)
+
+    def fused():
+        mkf_b200.field_bpfd(f, [0.0], mkf_b200.BMC_GT, out=out, stream=stream)
+
+    pbm0, _, _ = mkf_b200.bin_map_cuda(f, ">", 0.0)  # the map buffer, allocated once
+
+    def dropin():
+        pbm, org, _ = mkf_b200.bin_map_cuda(f, ">", 0.0, out=pbm0)
+        mkf_b200.get_bpfd(pbm, org, out=out[0])
+
+    res = {"workload": "256^3 FP32 ball (100 - |x - c| + U[-0.5, 0.5) noise), threshold 0, '>'",
+           "l2": "flushed before each call"}
+    for name, fn in (("fused", fused), ("dropin_pair", dropin)):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        ms = []
+        for _ in range(steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        med = float(np.median(ms))
+        res[name] = {"ms_per_call": med, "gvoxel_per_s": n / med * 1e-6}
+    del f, flush, pbm0
+    torch.cuda.empty_cache()
+    return res
 
 
 def run_serving_workload(dev, rates=(100, 500, 1000, 2000, 5000), max_requests=10000, seconds=3.0,
@@ -541,6 +587,86 @@ def cpu_baseline(f: np.ndarray, target_s: float = 10.0):
                       f"(16 reference calls), {dt:.2f} s"}
 
 
+def ball256_torch(device, seed=11):
+    """The plain method's workload: 256^3 FP32, 100 - |x - c| (c = 127.5 on each axis) plus
+    U[-0.5, 0.5) noise from a fixed seed; threshold 0, relation '>'."""
+    import torch
+
+    n, c = 256, 127.5
+    ax = torch.arange(n, dtype=torch.float64, device=device) - c
+    f = 100.0 - torch.sqrt(ax.view(-1, 1, 1) ** 2 + ax.view(1, -1, 1) ** 2 + ax.view(1, 1, -1) ** 2)
+    g = torch.Generator(device=device).manual_seed(seed)
+    f += torch.rand((n, n, n), dtype=torch.float64, device=device, generator=g) - 0.5
+    return f.float().contiguous()
+
+
+def reference_cuda(args):
+    """The reference's own CUDA path (binMapCUDA + mkfCUDAGetBPFD with the FAST profile, one call
+    pair per threshold as its one-threshold interface requires), compiled unmodified from its
+    sources for sm_100a, on the benchmark field resident in HBM and on the 256^3 FP32 ball.
+    Device-timed with CUDA events around each step; the reference synchronises after each of its
+    stages itself (utilCUDA.hpp:21-60), which is part of its cost."""
+    try:
+        import torch
+
+        if not torch.cuda.is_available():
+            return {"unavailable": "no CUDA device"}
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        from oracle import RefCuda
+    except Exception as e:  # noqa: BLE001 - reported, not fatal to the CPU arm
+        return {"unavailable": f"{type(e).__name__}: {e}"}
+    if not RefCuda.available():
+        return {"unavailable": "reference CUDA build (oracle/_ref/libmkfrefcuda.so) missing"}
+    ref = RefCuda()
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+
+    flush = torch.empty(64 << 20, dtype=torch.int32, device=dev)  # 256 MB > 126 MB L2
+
+    def timed(f, thresholds, workload, flush_l2):
+        Z, Y, X = f.shape
+        d = (X, Y, Z)
+        pbm = torch.empty(ref.pbm_words(d), dtype=torch.int32, device=dev)
+        counts = torch.zeros((len(thresholds), 256), dtype=torch.int64, device=dev)
+
+        def one():
+            counts.zero_()
+            return ref.bpfd(counts.data_ptr(), pbm.data_ptr(), f.data_ptr(), f.element_size(), d, thresholds, ">")
+
+        for _ in range(max(args.warmup, 1)):
+            one()
+        torch.cuda.synchronize(dev)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        t_map = t_bpfd = 0.0
+        for e0, e1 in ev:
+            if flush_l2:
+                flush.zero_()
+            e0.record(stream)
+            a, b = one()
+            e1.record(stream)
+            t_map += a
+            t_bpfd += b
+        torch.cuda.synchronize(dev)
+        ms = sum(e0.elapsed_time(e1) for e0, e1 in ev) / args.steps
+        return {"workload": workload, "ms_per_step": ms, "gvoxel_per_s": X * Y * Z / ms * 1e-6,
+                "map_ms_per_step": t_map / args.steps, "bpfd_ms_per_step": t_bpfd / args.steps,
+                "launches_per_step": 2 * len(thresholds),
+                "l2": "flushed before each step" if flush_l2 else "input larger than L2 (no flush)"}
+
+    out = {"build": "reference binMapCUDA.cu, mkfCUDA.cu, ctUtil.cu, gridUtil.cu (+ binMapUtil.c, encoding.c, "
+                    "geomSVU.c) compiled unmodified, nvcc -gencode arch=compute_100a,code=sm_100a -O3",
+           "thresholds": "rounded to float by the reference's interface (binMapUtil.c:37)"}
+    f = grf_torch(N_SIDE, N_SIDE, N_SIDE, SEED, dev)
+    out[WORKLOAD] = timed(f, THRESHOLDS, f"{N_SIDE}^3 FP64 GRF, {K_THRESH} thresholds (16 call pairs)", False)
+    del f
+    f = ball256_torch(dev)
+    out["ball256_f32_k1"] = timed(f, [0.0], "256^3 FP32 ball, threshold 0 (1 call pair)", True)
+    del f, flush
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -566,6 +692,8 @@ def run_reference(args, rank, world):
                          "sample": f"{planes} plane pairs x 1024 x 1024 FP64 GRF slab per step, 16 thresholds"},
         "e2e": {"value": value, "unit": "Gvoxel/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if not args.no_secondary:
+        line["reference_cuda"] = reference_cuda(args)
     print(json.dumps(line), flush=True)
 
 
@@ -691,6 +819,7 @@ def run_mkf(args, rank, world, local_rank):
         line["cpu_baseline"] = cpu_baseline(fh_np.reshape(-1))
     if world == 1 and not args.no_secondary:
         del fh, fh_np
+        line["plain"] = run_plain_workload(dev)
         line["batched"] = run_batch_workload(dev)
         line["serving"] = run_serving_workload(dev)
         line["insitu"] = run_insitu_workload(dev)

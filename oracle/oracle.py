@@ -7,6 +7,9 @@ this module; the product library never does.
   (``mkf_oracle.c``).
 * :class:`RefOracle` wraps ``_ref/libmkfref.so``, the reference MKF C path compiled from its own
   sources (``Makefile``). It exists only where it was built.
+* :class:`RefCuda` wraps ``_ref/libmkfrefcuda.so``, the reference MKF CUDA path
+  (``binMapCUDA`` + ``mkfCUDAGetBPFD``) compiled unmodified for sm_100a: a GPU cross-check and
+  the recompiled-reference timing point. It exists only where it was built.
 * :func:`bpfd_numpy` is a third, vectorised formulation used to cross-check the other two.
 """
 from __future__ import annotations
@@ -210,6 +213,59 @@ class RefOracle:
         sym = C.create_string_buffer(16)
         rv = self.L.mkfSelectMeasuresBPFD(m, sym, np.ascontiguousarray(h, np.uint64), s, pid)
         return rv, m, sym.raw[:12]
+
+
+class RefCuda:
+    """The reference MKF CUDA path, compiled unmodified from its .cu/.c sources for sm_100a
+    (oracle/Makefile, ref_cuda_harness.cu). All pointers are device addresses (ints)."""
+
+    PATH = os.path.join(HERE, "_ref", "libmkfrefcuda.so")
+
+    @classmethod
+    def available(cls) -> bool:
+        return os.path.exists(cls.PATH)
+
+    def __init__(self):
+        L = C.CDLL(self.PATH)
+        L.refcu_pbm_words.restype = C.c_size_t
+        L.refcu_pbm_words.argtypes = [C.POINTER(C.c_int)]
+        L.refcu_bpfd.restype = C.c_int
+        L.refcu_bpfd.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int),
+                                 np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS"), C.c_int, C.c_char_p,
+                                 C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        self.L = L
+
+    def pbm_words(self, def3) -> int:
+        """Words of the packed map binMapCUDA writes for def3 (setBMO, binMapUtil.c:60-87)."""
+        return int(self.L.refcu_pbm_words(_def(def3)))
+
+    def bpfd(self, counts_ptr: int, pbm_ptr: int, field_ptr: int, elem_bytes: int, def3, thresholds,
+             rel: str = ">"):
+        """One binMapCUDA + mkfCUDAGetBPFD call pair per threshold into counts_ptr + 256 k (u64,
+        zeroed by the caller). Thresholds pass through the reference's float parameter. Returns
+        the reference's own summed stage timings (map ms, BPFD ms)."""
+        t = np.ascontiguousarray(np.asarray(thresholds, np.float64).ravel())
+        ms_map, ms_bpfd = C.c_float(0), C.c_float(0)
+        ok = self.L.refcu_bpfd(C.c_void_p(counts_ptr), C.c_void_p(pbm_ptr), C.c_void_p(field_ptr),
+                               int(elem_bytes), _def(def3), t, int(t.size), rel.encode(),
+                               C.byref(ms_map), C.byref(ms_bpfd))
+        if not ok:
+            raise RuntimeError("reference CUDA path rejected the input or failed")
+        return ms_map.value, ms_bpfd.value
+
+    def bpfd_torch(self, field, thresholds, rel: str = ">"):
+        """Counts u64[K][256] (as a host numpy array) of a contiguous (Z, Y, X) FP32/FP64 CUDA
+        tensor by the reference CUDA path; X must be a multiple of 32."""
+        import torch
+
+        Z, Y, X = field.shape
+        d = (X, Y, Z)
+        pbm = torch.empty(self.pbm_words(d), dtype=torch.int32, device=field.device)
+        k = int(np.asarray(thresholds).size)
+        counts = torch.zeros((k, 256), dtype=torch.int64, device=field.device)
+        self.bpfd(counts.data_ptr(), pbm.data_ptr(), field.data_ptr(), field.element_size(), d, thresholds, rel)
+        torch.cuda.synchronize(field.device)
+        return counts.cpu().numpy().view(np.uint64)
 
 
 def bits_numpy(f: np.ndarray, t: float, m: int) -> np.ndarray:
