@@ -51,6 +51,14 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true", help="skip the batched, serving and in-situ workloads (and the reference CUDA point of the reference arm)")
+    ap.add_argument("--profile", choices=["field", "batch"], default=None,
+                    help="run one small case for a profiler instead of the benchmark: 'field' = one "
+                         "GRF (--side, --dtype, --thresholds), 'batch' = the uneven ball batch (--fields)")
+    ap.add_argument("--side", type=int, default=512)
+    ap.add_argument("--dtype", choices=["f32", "f64"], default="f64")
+    ap.add_argument("--thresholds", default="16", help="a count n (linspace(-2, 2, n)) or a comma list of values")
+    ap.add_argument("--fields", type=int, default=128)
+    ap.add_argument("--reps", type=int, default=2)
     return ap.parse_args()
 
 
@@ -230,46 +238,95 @@ def serving_pool(dev, n=48, seed=SEED + 4):
 
 
 def run_plain_workload(dev, steps=20, warmup=5):
-    """The plain method's workload (256^3 FP32 ball, threshold 0, '>'): the fused call
-    (mkfFieldBPFD) and the drop-in pair (binMapCUDA + mkfCUDAGetBPFD), field resident in HBM, L2
-    flushed before each call (the field is 67 MB, inside the 126 MB L2), CUDA events per call."""
+    """The plain method's workload (256^3 FP32 ball, threshold 0, '>'), field resident in HBM, L2
+    flushed before each call (the field is 67 MB, inside the 126 MB L2):
+
+    * fused: mkfFieldBPFD, CUDA events around each call with the queue kept busy (device time)
+      and with a synchronize after each call (the latency a caller sees through the Python API);
+    * dropin_pair: binMapCUDA + mkfCUDAGetBPFD called through the C ABI with their arguments built
+      once, as a C caller of the original makes them; time per pair including the host
+      synchronisation the original's per-stage timers impose, and the two stage times the
+      library reports in KernInfo (the same quantities the reference CUDA point reports)."""
+    import ctypes as C
+
     import torch
 
     import mkf_b200
+    from mkf_b200 import _lib
 
     f = ball256_torch(dev)
     n = f.numel()
+    Z, Y, X = f.shape
     stream = torch.cuda.current_stream(dev)
-    flush = torch.empty(64 << 20, dtype=torch.int32, device=dev)
+    flush = torch.empty(128 << 20, dtype=torch.int32, device=dev)  # 512 MB
     out = torch.zeros((1, 256), dtype=torch.int64, device=dev)
+    res = {"workload": "256^3 FP32 ball (100 - |x - c| + U[-0.5, 0.5) noise), threshold 0, '>'",
+           "l2": "flushed before each call"}
 
     def fused():
         mkf_b200.field_bpfd(f, [0.0], mkf_b200.BMC_GT, out=out, stream=stream)
 
-    pbm0, _, _ = mkf_b200.bin_map_cuda(f, ">", 0.0)  # the map buffer, allocated once
-
-    def dropin():
-        pbm, org, _ = mkf_b200.bin_map_cuda(f, ">", 0.0, out=pbm0)
-        mkf_b200.get_bpfd(pbm, org, out=out[0])
-
-    res = {"workload": "256^3 FP32 ball (100 - |x - c| + U[-0.5, 0.5) noise), threshold 0, '>'",
-           "l2": "flushed before each call"}
-    for name, fn in (("fused", fused), ("dropin_pair", dropin)):
-        for _ in range(warmup):
-            fn()
+    for _ in range(warmup):
+        fused()
+    torch.cuda.synchronize(dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for e0, e1 in ev:
+        flush.zero_()
+        e0.record(stream)
+        fused()
+        e1.record(stream)
+    torch.cuda.synchronize(dev)
+    dev_ms = float(np.median([e0.elapsed_time(e1) for e0, e1 in ev]))
+    api = []
+    for _ in range(steps):
+        flush.zero_()
         torch.cuda.synchronize(dev)
-        ms = []
-        for _ in range(steps):
-            flush.zero_()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            fn()
-            e1.record(stream)
-            e1.synchronize()
-            ms.append(e0.elapsed_time(e1))
-        med = float(np.median(ms))
-        res[name] = {"ms_per_call": med, "gvoxel_per_s": n / med * 1e-6}
-    del f, flush, pbm0
+        t0 = time.perf_counter()
+        fused()
+        torch.cuda.synchronize(dev)
+        api.append((time.perf_counter() - t0) * 1e3)
+    api_ms = float(np.median(api))
+    res["fused"] = {"device_ms_per_call": dev_ms, "gvoxel_per_s": n / dev_ms * 1e-6, "api_ms_per_call": api_ms}
+
+    L = mkf_b200.lib()
+    defs = (C.c_int * 3)(X, Y, Z)
+    table = (_lib.ConstFieldPtr * 4)()
+    table[0].p = f.data_ptr()
+    fi = _lib.BMFieldInfo()
+    fi.fieldTableMask = 1
+    fi.elemID = _lib.ENC_F32
+    fi.profID = 0
+    fi.pD = defs
+    fi.pFieldDevPtrTable = table
+    bm = _lib.BinMapF64()
+    L.setBinMapF64(C.byref(bm), b">", 0.0)
+    org = _lib.BMOrg()
+    ki = _lib.KernInfo()
+    pbm = torch.empty(int(L.setBMO(None, defs, bytes([0]))), dtype=torch.int32, device=dev)
+
+    def pair():
+        if not L.binMapCUDA(C.byref(ki), pbm.data_ptr(), C.byref(org), C.byref(fi), C.byref(bm)):
+            raise RuntimeError("binMapCUDA returned NULL")
+        L.mkfCUDAGetBPFD(C.byref(ki), out.data_ptr(), C.byref(org), pbm.data_ptr(), _lib.MKFCU_PROFILE_FAST)
+        return ki.dtms[0], ki.dtms[1]
+
+    for _ in range(warmup):
+        pair()
+    torch.cuda.synchronize(dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    t_map = t_cnt = 0.0
+    for e0, e1 in ev:
+        flush.zero_()
+        e0.record(stream)
+        a, b = pair()
+        e1.record(stream)
+        t_map += a
+        t_cnt += b
+    torch.cuda.synchronize(dev)
+    ms = float(np.median([e0.elapsed_time(e1) for e0, e1 in ev]))
+    res["dropin_pair"] = {"ms_per_pair": ms, "gvoxel_per_s": n / ms * 1e-6, "map_ms": t_map / steps,
+                          "bpfd_ms": t_cnt / steps}
+    del f, flush, pbm
     torch.cuda.empty_cache()
     return res
 
@@ -826,8 +883,57 @@ def run_mkf(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def run_profile_case(args):
+    """A small case for a profiler: 3 untimed launches, then --reps launches timed with CUDA
+    events; prints one JSON line (not a benchmark result)."""
+    import torch
+
+    import mkf_b200
+
+    dev = torch.device("cuda:0")
+    mkf_b200.lib()
+    if args.profile == "field":
+        n = args.side
+        f = grf_torch(n, n, n, 1, dev)
+        f = f if args.dtype == "f64" else f.float().contiguous()
+        t = (np.linspace(-2.0, 2.0, int(args.thresholds)) if "," not in args.thresholds and "." not in args.thresholds
+             else np.array([float(v) for v in args.thresholds.split(",")]))
+        out = torch.zeros((len(t), 256), dtype=torch.int64, device=dev)
+
+        def launch():
+            mkf_b200.field_bpfd(f, t, mkf_b200.BMC_GT, out=out)
+
+        vox, nbytes, what = f.numel(), f.numel() * f.element_size(), f"{n}^3 {args.dtype} GRF, {len(t)} thresholds"
+    else:
+        fields = ball_fields(args.fields, 77, dev)
+        plan = mkf_b200.BatchPlan(fields, [[0.0]] * len(fields))  # tunes the slab depth at creation
+
+        def launch():
+            plan.launch()
+
+        vox = sum(x.numel() for x in fields)
+        nbytes, what = vox * 4, f"{len(fields)} FP32 ball fields, threshold 0"
+    for _ in range(3):
+        launch()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.reps):
+        launch()
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / args.reps
+    print(json.dumps({"profile_case": what, "ms_per_launch": ms, "gvoxel_per_s": vox / ms * 1e-6,
+                      "field_gb_per_s": nbytes / ms * 1e-6}), flush=True)
+    if args.profile == "batch":
+        plan.close()
+
+
 def main():
     args = parse()
+    if args.profile:
+        run_profile_case(args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

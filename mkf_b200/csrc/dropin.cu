@@ -38,31 +38,49 @@ struct PackArgs
    long long nWords;       // rowWS * Y * Z
 };
 
-// One warp per packed word: lane j thresholds element x = 32*w + j (the sum of the fields) and
-// a ballot assembles the word. Loads are coalesced along x for planar fields.
+// One warp per row (y, z) of the map: lane j thresholds element x = 32 w + j (the sum of the
+// fields) of word w, four words per step with their loads issued together, and a ballot
+// assembles each word; lanes 0..3 store the step's words. Loads are coalesced along x for planar
+// fields; elements past the row end are not read (their bits are 0).
 template <typename T>
 __global__ void __launch_bounds__(256) packMap(const __grid_constant__ PackArgs a)
 {
+   constexpr int U = 4;
    const int lane = threadIdx.x & 31;
    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+   const long long nRows = (long long)a.Y * a.Z;
    const T t = (T)a.t;
    const T *f0 = (const T *)a.f[0];
-   for (long long i = gw; i < a.nWords; i += nw) {
-      const long long row = i / a.rowWS;
-      const int wi = (int)(i - row * a.rowWS);
-      const int y = (int)(row % a.Y);
+   for (long long row = gw; row < nRows; row += nw) {
       const int z = (int)(row / a.Y);
-      const int x = 32 * wi + lane;
-      unsigned bit = 0;
-      if (x < a.X) {
-         const long long off = (long long)x * a.sx + (long long)y * a.sy + (long long)z * a.sz;
-         T v = __ldg(f0 + off);
-         for (int k = 1; k < a.nF; k++) { v += __ldg((const T *)a.f[k] + off); }
-         bit = (a.m >> relIdx(v, t)) & 1u;
+      const int y = (int)(row - (long long)z * a.Y);
+      const long long base = (long long)y * a.sy + (long long)z * a.sz;
+      uint32_t *wrow = a.w + (size_t)z * a.planeWS + (size_t)y * a.rowWS;
+      for (int w0 = 0; w0 < (int)a.rowWS; w0 += U) {
+         T v[U];
+         bool in[U];
+#pragma unroll
+         for (int u = 0; u < U; u++) {
+            const int x = 32 * (w0 + u) + lane;
+            in[u] = x < a.X;
+            v[u] = in[u] ? __ldg(f0 + base + (long long)x * a.sx) : T(0);
+         }
+         for (int k = 1; k < a.nF; k++) {
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+               const int x = 32 * (w0 + u) + lane;
+               if (in[u]) { v[u] += __ldg((const T *)a.f[k] + base + (long long)x * a.sx); }
+            }
+         }
+         uint32_t mine = 0;
+#pragma unroll
+         for (int u = 0; u < U; u++) {
+            const uint32_t word = __ballot_sync(FULL, in[u] ? (a.m >> relIdx(v[u], t)) & 1u : 0u);
+            mine = (lane == u) ? word : mine;
+         }
+         if (lane < U && w0 + lane < (int)a.rowWS) { wrow[w0 + lane] = mine; }
       }
-      const uint32_t word = __ballot_sync(FULL, bit);
-      if (lane == 0) { a.w[(size_t)z * a.planeWS + (size_t)y * a.rowWS + wi] = word; }
    }
 }
 
@@ -240,7 +258,7 @@ MKF_API BMPackWord *binMapCUDA(KernInfo *pK, BMPackWord *pW, BMOrg *pO, const BM
    a.w = pW;
    a.nWords = (long long)org.rowWS * a.Y * a.Z;
    EventTimer tm;
-   long long grid = (a.nWords * 32 + 255) / 256;
+   long long grid = ((long long)a.Y * a.Z + 7) / 8;  // a warp per row
    const long long cap = (long long)smCount() * 16;
    if (grid > cap) { grid = cap; }
    if (pF->elemID == ENC_F32) { packMap<float><<<(unsigned)grid, 256>>>(a); }

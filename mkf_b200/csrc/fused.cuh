@@ -110,6 +110,9 @@ int planBatchField(const MKFFieldDesc *pF, const MKFThreshSet *pT, int rowBase, 
 // (tune.cu): the depth mkfTune measured best for this kind of field, else `def`.
 enum { kFamWords = 0, kFamThermo = 1 };
 int tunedDepth(int family, int enc, int K, int X, int Y, int Z, int def);
+// The untuned slab depth: def halved (down to 4) until a field of itemsPerPlane work items per
+// plane and Z planes has at least minItems items.
+int sizeDepth(int def, long long itemsPerPlane, int Z, long long minItems);
 // Whether mkfBatchPlanCreate measures the slab depth of each new plan (tune.cu).
 bool batchTuning();
 

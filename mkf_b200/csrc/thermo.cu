@@ -36,11 +36,14 @@ static constexpr int kThWarps = 8;
 #ifndef THERMO_D
 #define THERMO_D 64  // default planes of cells per work item
 #endif
+// Untuned fields get at least this many work items per SM (the slab depth is halved until they
+// do): measured on 128^3 to 512^3 fields with 16 thresholds.
+static constexpr int kThItemsPerSM = 14;
 #ifndef THERMO_BATCH_MINB
 #define THERMO_BATCH_MINB 2  // the per-field variant switch needs the larger register budget
 #endif
-static constexpr int kThSlots = 3;
-static constexpr int kThMaxDepth = 255;  // planes per work item the all-ones counters can hold  // predicated mixed-code slots per cell (K > 1)
+static constexpr int kThSlots = 3;       // unpredicated mixed-code slots per cell (K > 1)
+static constexpr int kThMaxDepth = 255;  // planes per work item the all-ones counters can hold
 static constexpr int kLutShift = 18;
 static constexpr int kLutSize = 1 << (32 - kLutShift);
 
@@ -90,7 +93,7 @@ __device__ __noinline__ uint32_t exactRank(const T *__restrict__ F, long long i,
 template <int NROW>
 struct PlaneOnes
 {
-   static_assert(NROW == 8 || NROW == 16, "tree of 8 or 16 rows");
+   static_assert(NROW == 4 || NROW == 8 || NROW == 16, "tree of 4, 8 or 16 rows");
    uint32_t ones = 0, twos = 0, fours = 0, eights = 0;
    // bit-sliced counts of the NROW-weight carries: at most one carry per plane, so an item of up
    // to kThMaxDepth planes needs 8 slices (a 6-slice count wraps at 64 planes of all-ones cells)
@@ -118,6 +121,7 @@ struct PlaneOnes
       fa(ones, c2, ones, p1, w);
       if ((J & 2) == 0) { p2 = c2; return; }
       fa(twos, c4, twos, p2, c2);
+      if (NROW == 4) { ripple(c4); return; }
       if ((J & 4) == 0) { p4 = c4; return; }
       fa(fours, c8, fours, p4, c4);
       if (NROW == 8) { ripple(c8); return; }
@@ -605,7 +609,9 @@ int launchThermo(FusedArgs &a, int enc, cudaStream_t s)
 {
    a.lutC = prepareKeys(a, enc);
    if (a.lutC == 0) { return MKF_ERR_UNSUPPORTED; }
-   itemGrid(a, tunedDepth(kFamThermo, enc, a.K, a.X, a.Y, a.Z, THERMO_D));
+   const long long perPlane = (long long)((a.X - 1 + 30) / 31) * ((a.Y - 1 + THERMO_TY - 1) / THERMO_TY);
+   itemGrid(a, tunedDepth(kFamThermo, enc, a.K, a.X, a.Y, a.Z,
+                          sizeDepth(THERMO_D, perPlane, a.Z, (long long)smCount() * kThItemsPerSM)));
    const bool ge = a.rankHi != 0, inner = innerTiles(a, enc);
    if (enc == ENC_F32) { return ge ? launchThermoG<float, true>(a, inner, s) : launchThermoG<float, false>(a, inner, s); }
    return ge ? launchThermoG<double, true>(a, inner, s) : launchThermoG<double, false>(a, inner, s);

@@ -49,6 +49,13 @@ int tunedDepth(int family, int enc, int K, int X, int Y, int Z, int def)
    return it == gTuned.end() ? def : it->second;
 }
 
+int sizeDepth(int def, long long itemsPerPlane, int Z, long long minItems)
+{
+   int D = def;
+   while (D > 4 && itemsPerPlane * ((Z - 1 + D - 1) / D) < minItems) { D >>= 1; }
+   return D;
+}
+
 bool batchTuning()
 {
    std::lock_guard<std::mutex> lk(gTuneMu);
@@ -79,11 +86,11 @@ MKF_API int mkfTune(const MKFFieldDesc *pF, const MKFThreshSet *pT, void *stream
    if (e == cudaSuccess) { e = cudaEventCreate(&e0); }
    if (e == cudaSuccess) { e = cudaEventCreate(&e1); }
    int rc = (e == cudaSuccess) ? MKF_OK : cudaFail(e, "mkfTune: set-up");
-   static const int kCand[] = {8, 16, 32, 64, 128};
+   static const int kCand[] = {4, 8, 16, 32, 64, 128};
    float best = 0.0f;
    int bestD = 0;
    std::vector<TuneKey> seen;
-   for (int c = 0; c < 5 && rc == MKF_OK; c++) {
+   for (int c = 0; c < 6 && rc == MKF_OK; c++) {
       tForce = kCand[c];
       tSeen = &seen;
       seen.clear();

@@ -27,6 +27,10 @@ static constexpr int kWdWarps = 8;
 #define WORDS_D 32
 #endif
 static constexpr int kWdD = WORDS_D;  // default planes of cells per work item (WordTask::D)
+// Untuned fields get at least this many work items per SM (the slab depth is halved until they
+// do): measured on 256^3 to 512^3 fields, fewer items than ~0.6 of the resident warps leave SMs
+// idle while deeper items win nothing.
+static constexpr int kWdItemsPerSM = 20;
 
 // Relation class of a threshold: every class is one comparison (NaN maps as the EQ bit says).
 enum WordCls { kGT = 0, kGE = 1, kLT = 2, kLE = 3, kGEN = 4 };
@@ -372,7 +376,8 @@ int launchWords(const FusedArgs &f, int enc, const uint32_t *masks, cudaStream_t
    }
    a.nChunkX = (a.X - 1 + 30) / 31;
    a.nTileY = (a.Y - 1 + 30) / 31;
-   a.D = tunedDepth(kFamWords, enc, a.K, a.X, a.Y, a.Z, kWdD);
+   a.D = tunedDepth(kFamWords, enc, a.K, a.X, a.Y, a.Z,
+                    sizeDepth(kWdD, (long long)a.nChunkX * a.nTileY, a.Z, (long long)smCount() * kWdItemsPerSM));
    a.nSlabZ = (a.Z - 1 + a.D - 1) / a.D;
    a.nItems = (long long)a.nChunkX * a.nTileY * a.nSlabZ;
    if (enc == ENC_F32) { return dispatchWords<float>(a, s); }
@@ -422,7 +427,7 @@ int launchWordsMoments(const FusedArgs &f, int enc, const uint32_t *masks, doubl
    }
    a.nChunkX = (a.X - 1 + 30) / 31;
    a.nTileY = (a.Y - 1 + 30) / 31;
-   a.D = kWdD;
+   a.D = sizeDepth(kWdD, (long long)a.nChunkX * a.nTileY, a.Z, (long long)smCount() * kWdItemsPerSM);
    a.nSlabZ = (a.Z - 1 + a.D - 1) / a.D;
    a.nItems = (long long)a.nChunkX * a.nTileY * a.nSlabZ;
    const int64_t syb = a.sy * (enc == ENC_F32 ? 4 : 8);
