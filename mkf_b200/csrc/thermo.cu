@@ -164,9 +164,10 @@ static constexpr int kHistRow = THERMO_HROW;
 #define THERMO_HCOPIES 2
 #endif
 static constexpr int kHistCopies = THERMO_HCOPIES;
+// (plus per-lane scratch words after it, 32 + 2 rows: an empty slot q adds to scratch + q rows)
 __host__ __device__ constexpr size_t thermoDynBytes(int K)
 {
-   return ((size_t)K * kHistRow * kHistCopies + 32) * sizeof(uint32_t);
+   return ((size_t)K * kHistRow * kHistCopies + 32 + 2 * kHistRow) * sizeof(uint32_t);
 }
 
 // Load one field's thresholds, build its rank table and clear the histogram (whole CTA).
@@ -251,6 +252,19 @@ __device__ __forceinline__ void redShared(uint32_t addr)
 {
    asm volatile("red.shared.add.u32 [%0], 1;" ::"r"(addr) : "memory");
 }
+
+// The same at byte address addr + OFF (the offset rides in the instruction).
+template <int OFF>
+__device__ __forceinline__ void redSharedAt(uint32_t addr)
+{
+   asm volatile("red.shared.add.u32 [%0+%1], 1;" ::"r"(addr), "n"(OFF) : "memory");
+}
+
+// Gather eight bits of t into an 8-bit code with one multiply: for bit 0 of every byte of the
+// first corner word at bits 0, 8, 16, 24 and of the second at bits 4, 12, 20, 28, the multiplier
+// 0x01020408 moves them to bits 24..31 in corner order; for bit 1 (positions one higher)
+// 0x00810204 does. No two partial products meet below bit 32, so no carry reaches the code.
+__device__ __forceinline__ uint32_t gatherBits(uint32_t t, uint32_t mul) { return (t * mul) >> 24; }
 
 // Pattern of a cell for threshold k from its two faces' packed corner ranks R0 (plane z) and R1
 // (plane z + 1), C = 0x7F7F7F7F - k * 0x01010101: adding C sets a byte's top bit iff its rank
@@ -388,17 +402,19 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
             const uint32_t R0 = sF[j], R1 = fc;
             const uint32_t spread = rmax - rmin;
             const uint32_t rowAddr = hist32 + rmin * (kHistRow * 4);
-            const uint32_t rb = rmin * 0x01010101u;
-            const uint32_t D0 = R0 - rb, D1 = R1 - rb;
-            const uint32_t b0 = gatherCode(((D0 << 3) & 0x08080808u) | ((D1 << 7) & 0x80808080u));
+            // integer multiply-adds (not shifts and logic) where they serve: the kernel is bound by
+            // the integer ALU pipe, and these run on the FMA pipe
+            const uint32_t D0 = R0 + rmin * 0xFEFEFEFFu;         // R0 - rmin per byte (no borrows)
+            const uint32_t D1s = R1 * 16u + rmin * 0xEFEFEFF0u;  // (R1 - rmin per byte) << 4
+            const uint32_t b0 = gatherBits((D0 & 0x01010101u) | (D1s & 0x10101010u), 0x01020408u);
             if (NSLOT == 1) {
                redShared(spread != 0 ? rowAddr + (b0 << 2) : trash);
             } else {
-               const uint32_t b1 = gatherCode(((D0 << 2) & 0x08080808u) | ((D1 << 6) & 0x80808080u));
+               const uint32_t b1 = gatherBits((D0 & 0x02020202u) | (D1s & 0x20202020u), 0x00810204u);
                const bool fast = spread < 4;
-               redShared(fast && spread > 0 ? rowAddr + ((b0 | b1) << 2) : trash);
-               redShared(fast && spread > 1 ? rowAddr + kHistRow * 4 + (b1 << 2) : trash);
-               redShared(fast && spread > 2 ? rowAddr + kHistRow * 8 + ((b0 & b1) << 2) : trash);
+               redSharedAt<0>(fast && spread > 0 ? (b0 | b1) * 4u + rowAddr : trash);
+               redSharedAt<kHistRow * 4>(fast && spread > 1 ? b1 * 4u + rowAddr : trash);
+               redSharedAt<kHistRow * 8>(fast && spread > 2 ? (b0 & b1) * 4u + rowAddr : trash);
                if (!fast) {  // counted after the row loop: one copy of that code, not one per row
                   wq[nwq] = make_uint4(R0, R1, rmin, rmax);
                   ++nwq;
