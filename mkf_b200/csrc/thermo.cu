@@ -263,7 +263,8 @@ __device__ __forceinline__ void redSharedAt(uint32_t addr)
 // Gather eight bits of t into an 8-bit code with one multiply: for bit 0 of every byte of the
 // first corner word at bits 0, 8, 16, 24 and of the second at bits 4, 12, 20, 28, the multiplier
 // 0x01020408 moves them to bits 24..31 in corner order; for bit 1 (positions one higher)
-// 0x00810204 does. No two partial products meet below bit 32, so no carry reaches the code.
+// 0x00810204 does, for bit 2 0x00408102. No two partial products meet below bit 32, so no carry
+// reaches the code.
 __device__ __forceinline__ uint32_t gatherBits(uint32_t t, uint32_t mul) { return (t * mul) >> 24; }
 
 // Pattern of a cell for threshold k from its two faces' packed corner ranks R0 (plane z) and R1
@@ -397,8 +398,8 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
             // Mixed codes, k = rmin .. rmax - 1. With d = corner rank - rmin per byte, the code
             // for k = rmin + q marks the corners with d > q; with b0, b1 the masks of corners
             // whose d has bit 0, 1 set, the codes for a spread rmax - rmin up to 3 are b0 | b1,
-            // b1, b0 & b1. Wider cells (about 1 in 100) are queued and count their codes one
-            // threshold at a time after the row loop.
+            // b1, b0 & b1. Wider cells (1 in 100 on a unit-variance field with thresholds 0.27
+            // apart) are queued and counted after the row loop.
             const uint32_t R0 = sF[j], R1 = fc;
             const uint32_t spread = rmax - rmin;
             const uint32_t rowAddr = hist32 + rmin * (kHistRow * 4);
@@ -427,14 +428,32 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
          mnPrev = mn;
          mxPrev = mx;
       }
-      // wide cells: every code k = rmin .. rmax - 1 from the packed corner ranks
+      // wide cells: every code k = rmin .. rmax - 1 from the packed corner ranks, by seven fixed
+      // formulas up to a spread of 7 (no loop whose trip count differs between lanes)
       for (int i = 0; i < nwq; ++i) {
          const uint32_t R0 = wq[i].x, R1 = wq[i].y, rmin = wq[i].z, rmax = wq[i].w;
-         uint32_t C = 0x7F7F7F7Fu - rmin * 0x01010101u, addr = hist32 + rmin * (kHistRow * 4);
-         for (uint32_t k = rmin; k < rmax; ++k) {
-            redShared(addr + (cellCode(R0, R1, C) << 2));
-            C -= 0x01010101u;
-            addr += kHistRow * 4;
+         const uint32_t spread = rmax - rmin, rowAddr = hist32 + rmin * (kHistRow * 4);
+         if (spread < 8) {
+            // d = corner rank - rmin < 8: with b0, b1, b2 the masks of corners whose d has bit 0,
+            // 1, 2 set, the code for k = rmin + q (corners with d > q) is one formula per q
+            const uint32_t D0 = R0 + rmin * 0xFEFEFEFFu, D1s = R1 * 16u + rmin * 0xEFEFEFF0u;
+            const uint32_t b0 = gatherBits((D0 & 0x01010101u) | (D1s & 0x10101010u), 0x01020408u);
+            const uint32_t b1 = gatherBits((D0 & 0x02020202u) | (D1s & 0x20202020u), 0x00810204u);
+            const uint32_t b2 = gatherBits((D0 & 0x04040404u) | (D1s & 0x40404040u), 0x00408102u);
+            redSharedAt<0>((b0 | b1 | b2) * 4u + rowAddr);  // spread >= 4: codes q = 0..3 all count
+            redSharedAt<kHistRow * 4>((b1 | b2) * 4u + rowAddr);
+            redSharedAt<kHistRow * 8>((b2 | (b1 & b0)) * 4u + rowAddr);
+            redSharedAt<kHistRow * 12>(b2 * 4u + rowAddr);
+            redSharedAt<kHistRow * 16>(spread > 4 ? (b2 & (b1 | b0)) * 4u + rowAddr : trash - kHistRow * 16);
+            redSharedAt<kHistRow * 20>(spread > 5 ? (b2 & b1) * 4u + rowAddr : trash - kHistRow * 20);
+            redSharedAt<kHistRow * 24>(spread > 6 ? (b2 & b1 & b0) * 4u + rowAddr : trash - kHistRow * 24);
+         } else {
+            uint32_t C = 0x7F7F7F7Fu - rmin * 0x01010101u, addr = rowAddr;
+            for (uint32_t k = rmin; k < rmax; ++k) {
+               redShared(addr + (cellCode(R0, R1, C) << 2));
+               C -= 0x01010101u;
+               addr += kHistRow * 4;
+            }
          }
       }
    }

@@ -591,3 +591,31 @@ def test_full_size_smooth_field_two_kernels_agree(mkf, cuda):
             assert (u64(mkf.field_bpfd(f, t[k:k + 1], mkf.BMC_GT))[0] == h[k]).all(), (tuned, k)
     del f
     torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_dense_thresholds_on_a_smooth_field(mkf, oracle, cuda, dtype):
+    """A smooth Gaussian field (sigma 4) with thresholds closer than its cell-to-cell variation
+    (32 over [-2, 2], 16 over [-1, 1]): many cells span 4 to 7 thresholds and some 8 or more, the
+    cases the rank-table kernel counts after its row loop. Whole tiles (X >= 32), single-field and
+    batched, against the oracle."""
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    if repo not in sys.path:
+        sys.path.insert(0, repo)
+    import bench
+
+    import torch
+
+    g = bench.grf_torch(64, 72, 160, 13, cuda)
+    fd = g.to(torch.float64 if dtype == np.float64 else torch.float32).contiguous()
+    f = fd.cpu().numpy()
+    Z, Y, X = f.shape
+    ths = [list(np.linspace(-2, 2, 32)), list(np.linspace(-1, 1, 16))]
+    want = []
+    for t in ths:
+        w = oracle.bpfd_field(f, (X, Y, Z), t, mkf.BMC_GT)
+        assert (u64(mkf.field_bpfd(fd, t, mkf.BMC_GT)) == w).all(), len(t)
+        want.append(w)
+    plan = mkf.BatchPlan([fd, fd], ths)
+    assert (u64(plan.launch()) == np.concatenate(want)).all()
+    plan.close()
