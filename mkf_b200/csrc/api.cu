@@ -134,11 +134,11 @@ struct MKFBatchPlan
    FieldTask *dTasks[2] = {nullptr, nullptr};  // thermometer-kernel fields, FP32 and FP64
    BatchChunk *dChunks[2] = {nullptr, nullptr};
    int nChunks[2] = {0, 0};
-   int maxK[2] = {0, 0};
+   std::vector<ThermoGroup> groups[2];  // the thermometer chunks of each kernel variant
    WordTask *dWTasks[2] = {nullptr, nullptr};  // word-kernel fields, FP32 and FP64
    BatchChunk *dWChunks[2] = {nullptr, nullptr};
    int nWChunks[2] = {0, 0};
-   unsigned *dCounter = nullptr;    // chunk counters: words FP32, words FP64, thermometer FP32, FP64
+   unsigned *dCounter = nullptr;  // chunk counters: words FP32, FP64, then thermometer FP32, FP64 per variant
    std::vector<ConstEntry> consts;
    std::vector<unsigned long long> constCells;
    struct Fallback
@@ -156,6 +156,7 @@ struct MKFBatchPlan
 };
 
 static constexpr int kChunkItems = 64;
+static constexpr int kPlanCounters = 2 + 2 * kThVariants;
 
 static void freePlan(MKFBatchPlan *p)
 {
@@ -215,7 +216,6 @@ static int createPlan(MKFBatchPlan **pp, uint64_t *pBPFD, const MKFFieldDesc *pF
          }
          t.out = pBPFD;
          tasks[e].push_back(t);
-         p->maxK[e] = std::max(p->maxK[e], t.K);
       } else if (cells > 0 && varying) {
          MKFBatchPlan::Fallback fb;
          fb.d = *d;
@@ -232,9 +232,10 @@ static int createPlan(MKFBatchPlan **pp, uint64_t *pBPFD, const MKFFieldDesc *pF
       row += (size_t)ts->nT;
    }
    p->rows = row;
-   cudaError_t e = cudaMalloc(&p->dCounter, 4 * sizeof(unsigned));
+   cudaError_t e = cudaMalloc(&p->dCounter, kPlanCounters * sizeof(unsigned));
    for (int k = 0; k < 2 && e == cudaSuccess; k++) {
       if (tasks[k].empty()) { continue; }
+      p->groups[k] = groupThermoChunks(chunks[k], tasks[k]);
       e = cudaMalloc(&p->dTasks[k], tasks[k].size() * sizeof(FieldTask));
       if (e == cudaSuccess) { e = cudaMalloc(&p->dChunks[k], chunks[k].size() * sizeof(BatchChunk)); }
       if (e == cudaSuccess) { e = cudaMemcpy(p->dTasks[k], tasks[k].data(), tasks[k].size() * sizeof(FieldTask), cudaMemcpyHostToDevice); }
@@ -267,7 +268,7 @@ static int planLaunchOn(MKFBatchPlan *p, cudaStream_t s)
       rc = launchConstBin(p->out, p->consts[i].row, p->consts[i].bin, p->constCells[i], s);
    }
    if (rc == MKF_OK && (p->nChunks[0] > 0 || p->nChunks[1] > 0 || p->nWChunks[0] > 0 || p->nWChunks[1] > 0)) {
-      e = cudaMemsetAsync(p->dCounter, 0, 4 * sizeof(unsigned), s);
+      e = cudaMemsetAsync(p->dCounter, 0, kPlanCounters * sizeof(unsigned), s);
       if (e != cudaSuccess) { return cudaFail(e, "batch counter clear"); }
    }
    for (int k = 0; k < 2 && rc == MKF_OK; k++) {
@@ -281,12 +282,8 @@ static int planLaunchOn(MKFBatchPlan *p, cudaStream_t s)
    }
    for (int k = 0; k < 2 && rc == MKF_OK; k++) {
       if (p->nChunks[k] == 0) { continue; }
-      BatchArgs b;
-      b.tasks = p->dTasks[k];
-      b.chunks = p->dChunks[k];
-      b.nChunks = p->nChunks[k];
-      b.counter = p->dCounter + 2 + k;
-      rc = launchThermoBatch(b, k == 0 ? ENC_F32 : ENC_F64, p->maxK[k], s);
+      rc = launchThermoGroups(p->dTasks[k], p->dChunks[k], p->groups[k], p->dCounter + 2 + k * kThVariants,
+                              k == 0 ? ENC_F32 : ENC_F64, s);
    }
    for (size_t i = 0; i < p->fallbacks.size() && rc == MKF_OK; i++) {
       const MKFBatchPlan::Fallback &fb = p->fallbacks[i];

@@ -120,7 +120,17 @@ bool batchTuning();
 bool prepareThermoTask(FieldTask &t, int enc, int depth = 0);
 // Launch the batched thermometer kernel over tasks of one element type (enc) whose largest
 // threshold count is maxK.
-int launchThermoBatch(const BatchArgs &b, int enc, int maxK, cudaStream_t s);
+// Chunks of one kernel variant of the batched rank-table kernel: [c0, c1) of the sorted chunk list.
+struct ThermoGroup
+{
+   int variant, c0, c1, maxK;
+};
+static constexpr int kThVariants = 16;  // variant indices 0..15 (FieldTask::variant & 13 is used)
+// Sort a batch's chunks by their field's variant (stable within a variant) and return the groups.
+std::vector<ThermoGroup> groupThermoChunks(std::vector<BatchChunk> &chunks, const std::vector<FieldTask> &tasks);
+// One launch per group; counters[v] (zeroed beforehand) hands out the chunks of variant v.
+int launchThermoGroups(const FieldTask *dTasks, const BatchChunk *dChunks, const std::vector<ThermoGroup> &groups,
+                       unsigned *counters, int enc, cudaStream_t s);
 
 // Fill a word task's relation classes, batched variant and item grid (words.cu); launch the
 // batched word kernel over the chunks of tasks of one element type.

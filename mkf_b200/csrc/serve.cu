@@ -24,6 +24,8 @@ using Clock = std::chrono::steady_clock;
 
 namespace mkf {
 
+static constexpr int kServerCounters = 2 + 2 * kThVariants;  // chunk counters per launch slot
+
 enum ReqState { kQueued, kRunning, kDone };
 
 struct Request
@@ -95,7 +97,7 @@ struct LaunchSlot
    std::vector<Request *> reqs;
    DevBuf work;      // tasks, chunks, clear list (uploaded each launch)
    DevBuf results;   // counts of requests that want them on the host
-   unsigned *counters = nullptr;  // 4 chunk counters: words FP32, FP64, thermometer FP32, FP64
+   unsigned *counters = nullptr;  // chunk counters: words FP32, FP64, then thermometer FP32, FP64 per variant
    bool busy = false;
 };
 
@@ -157,7 +159,6 @@ static int issueLaunch(MKFServer *s, LaunchSlot &sl)
    // plan every request: word tasks, thermometer tasks, constant maps, single-field fallbacks
    std::vector<FieldTask> tasks[2];
    std::vector<BatchChunk> chunks[2];
-   int maxK[2] = {0, 0};
    std::vector<WordTask> wtasks[2];
    std::vector<BatchChunk> wchunks[2];
    std::vector<ClearEntry> clears;
@@ -203,8 +204,11 @@ static int issueLaunch(MKFServer *s, LaunchSlot &sl)
          for (long long b = 0; b < t.nItems; b += kChunk) { chunks[k].push_back({f, 0, b, std::min<long long>(b + kChunk, t.nItems)}); }
          t.out = r->dCounts;
          tasks[k].push_back(t);
-         maxK[k] = std::max(maxK[k], t.K);
       }
+   }
+   std::vector<ThermoGroup> groups[2];  // thermometer chunks sorted into one run per kernel variant
+   for (int k = 0; k < 2; k++) {
+      if (!chunks[k].empty()) { groups[k] = groupThermoChunks(chunks[k], tasks[k]); }
    }
    // one upload of the whole work list, segments 256-byte aligned:
    // clears | thermometer tasks, chunks (FP32, FP64) | word tasks, chunks (FP32, FP64)
@@ -229,7 +233,9 @@ static int issueLaunch(MKFServer *s, LaunchSlot &sl)
       if (g.bytes) { memcpy(h + g.off, g.src, g.bytes); }
    }
    if ((e = cudaMemcpyAsync(dv, h, total, cudaMemcpyHostToDevice, st)) != cudaSuccess) { return cudaFail(e, "server: work list upload"); }
-   if ((e = cudaMemsetAsync(sl.counters, 0, 4 * sizeof(unsigned), st)) != cudaSuccess) { return cudaFail(e, "server: counters"); }
+   if ((e = cudaMemsetAsync(sl.counters, 0, kServerCounters * sizeof(unsigned), st)) != cudaSuccess) {
+      return cudaFail(e, "server: counters");
+   }
    if (!clears.empty()) {
       clearCounts<<<(unsigned)std::min<size_t>(clears.size(), 1024), 256, 0, st>>>((const ClearEntry *)(dv + seg[0].off), (int)clears.size());
       if ((e = cudaGetLastError()) != cudaSuccess) { return cudaFail(e, "server: clear launch"); }
@@ -249,12 +255,8 @@ static int issueLaunch(MKFServer *s, LaunchSlot &sl)
    }
    for (int k = 0; k < 2 && rc == MKF_OK; k++) {
       if (chunks[k].empty()) { continue; }
-      BatchArgs b;
-      b.tasks = (const FieldTask *)(dv + seg[1 + 2 * k].off);
-      b.chunks = (const BatchChunk *)(dv + seg[2 + 2 * k].off);
-      b.nChunks = (int)chunks[k].size();
-      b.counter = sl.counters + 2 + k;
-      rc = launchThermoBatch(b, k == 0 ? ENC_F32 : ENC_F64, maxK[k], st);
+      rc = launchThermoGroups((const FieldTask *)(dv + seg[1 + 2 * k].off), (const BatchChunk *)(dv + seg[2 + 2 * k].off),
+                              groups[k], sl.counters + 2 + k * kThVariants, k == 0 ? ENC_F32 : ENC_F64, st);
    }
    for (size_t i = 0; i < singles.size() && rc == MKF_OK; i++) {
       Request *r = singles[i].r;
@@ -427,7 +429,7 @@ MKF_API int mkfServerCreate(MKFServer **ps, const MKFServerConfig *cfg)
       if (e == cudaSuccess) { e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking); }
       if (e == cudaSuccess) { e = cudaEventCreateWithFlags(&sl.copied, cudaEventDisableTiming); }
       if (e == cudaSuccess) { e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming); }
-      if (e == cudaSuccess) { e = cudaMalloc(&sl.counters, 4 * sizeof(unsigned)); }
+      if (e == cudaSuccess) { e = cudaMalloc(&sl.counters, kServerCounters * sizeof(unsigned)); }
    }
    if (e != cudaSuccess) {
       const int rc = cudaFail(e, "mkfServerCreate");

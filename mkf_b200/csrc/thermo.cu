@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <vector>
 #include "fused.cuh"
 
 namespace mkf {
@@ -39,9 +40,6 @@ static constexpr int kThWarps = 8;
 // Untuned fields get at least this many work items per SM (the slab depth is halved until they
 // do): measured on 128^3 to 512^3 fields with 16 thresholds.
 static constexpr int kThItemsPerSM = 14;
-#ifndef THERMO_BATCH_MINB
-#define THERMO_BATCH_MINB 2  // the per-field variant switch needs the larger register budget
-#endif
 static constexpr int kThSlots = 3;       // unpredicated mixed-code slots per cell (K > 1)
 static constexpr int kThMaxDepth = 255;  // planes per work item the all-ones counters can hold
 static constexpr int kLutShift = 18;
@@ -483,9 +481,11 @@ __global__ void __launch_bounds__(kThWarps * 32, THERMO_MINB) thermoBPFD(const _
 // A CTA takes chunks of consecutive work items from a global counter; chunks never span fields.
 // When the next chunk belongs to another field, the CTA adds its counts of the previous field to
 // that field's output rows, then loads the new field's thresholds and rank table. One kernel per
-// element type keeps the per-field switch to four variants (relation, shifted edge items).
-template <typename T, int TY>
-__global__ void __launch_bounds__(kThWarps * 32, THERMO_BATCH_MINB) thermoBatch(const __grid_constant__ BatchArgs b)
+// element type and variant V (FieldTask::variant without its FP64 bit: bit 0 ">=", bit 2 shifted
+// edge items, bit 3 up to four rank-table candidates), so the counting loop is the single-field
+// kernel's, with its register budget; a batch launches one kernel per variant it holds.
+template <typename T, int TY, int V>
+__global__ void __launch_bounds__(kThWarps * 32, THERMO_MINB) thermoBatch(const __grid_constant__ BatchArgs b)
 {
    __shared__ ThermoShared S;
    __shared__ FieldTask F;
@@ -516,16 +516,7 @@ __global__ void __launch_bounds__(kThWarps * 32, THERMO_BATCH_MINB) thermoBatch(
          cur = ch.field;
       }
       for (long long it = ch.begin + warp; it < ch.end; it += kThWarps) {
-         switch (F.variant & 13) {
-            case 0: cells += warpItem<T, TY, false, kThSlots, false, 1>(F, it, S, sHist); break;
-            case 1: cells += warpItem<T, TY, true, kThSlots, false, 1>(F, it, S, sHist); break;
-            case 4: cells += warpItem<T, TY, false, kThSlots, true, 1>(F, it, S, sHist); break;
-            case 5: cells += warpItem<T, TY, true, kThSlots, true, 1>(F, it, S, sHist); break;
-            case 8: cells += warpItem<T, TY, false, kThSlots, false, 4>(F, it, S, sHist); break;
-            case 9: cells += warpItem<T, TY, true, kThSlots, false, 4>(F, it, S, sHist); break;
-            case 12: cells += warpItem<T, TY, false, kThSlots, true, 4>(F, it, S, sHist); break;
-            default: cells += warpItem<T, TY, true, kThSlots, true, 4>(F, it, S, sHist); break;
-         }
+         cells += warpItem<T, TY, (V & 1) != 0, kThSlots, (V & 4) != 0, (V & 8) ? 4 : 1>(F, it, S, sHist);
       }
    }
    if (cur >= 0) {
@@ -612,20 +603,74 @@ bool prepareThermoTask(FieldTask &t, int enc, int depth)
    return true;
 }
 
-int launchThermoBatch(const BatchArgs &b, int enc, int maxK, cudaStream_t s)
+std::vector<ThermoGroup> groupThermoChunks(std::vector<BatchChunk> &chunks, const std::vector<FieldTask> &tasks)
+{
+   std::vector<ThermoGroup> groups;
+   std::vector<BatchChunk> sorted;
+   sorted.reserve(chunks.size());
+   for (int v = 0; v < kThVariants; v++) {
+      ThermoGroup g{v, (int)sorted.size(), 0, 0};
+      for (const BatchChunk &c : chunks) {
+         const FieldTask &t = tasks[c.field];
+         if ((t.variant & 13) == v) {
+            sorted.push_back(c);
+            g.maxK = std::max(g.maxK, t.K);
+         }
+      }
+      g.c1 = (int)sorted.size();
+      if (g.c1 > g.c0) { groups.push_back(g); }
+   }
+   chunks.swap(sorted);
+   return groups;
+}
+
+template <typename T, int V>
+static int launchThermoBatchV(const BatchArgs &b, int maxK, cudaStream_t s)
 {
    constexpr int TY = THERMO_TY;
-   static std::atomic<int> occ[2][MKF_MAX_THRESH + 1];
-   const int e = enc == ENC_F32 ? 0 : 1;
-   auto kern = e == 0 ? thermoBatch<float, TY> : thermoBatch<double, TY>;
-   if (maxK < 1 || maxK > MKF_MAX_THRESH) { setError("thermoBatch: bad threshold count %d", maxK); return MKF_ERR_ARG; }
-   const size_t smem = thermoDynBytes(maxK);  // every field of the batch has at most maxK thresholds
-   const int blocksPerSM = cachedOccupancy(occ[e][maxK], kern, kThWarps * 32, smem, thermoDynBytes(MKF_MAX_THRESH));
+   static std::atomic<int> occ[MKF_MAX_THRESH + 1];
+   auto kern = thermoBatch<T, TY, V>;
+   const size_t smem = thermoDynBytes(maxK);  // every field of the group has at most maxK thresholds
+   const int blocksPerSM = cachedOccupancy(occ[maxK], kern, kThWarps * 32, smem, thermoDynBytes(MKF_MAX_THRESH));
    long long grid = (long long)smCount() * blocksPerSM;
    if (grid > b.nChunks) { grid = b.nChunks; }
    if (grid < 1) { grid = 1; }
    kern<<<(unsigned)grid, kThWarps * 32, smem, s>>>(b);
    return cudaFail(cudaGetLastError(), "thermoBatch launch");
+}
+
+template <typename T>
+static int launchThermoBatchT(const BatchArgs &b, int variant, int maxK, cudaStream_t s)
+{
+   switch (variant) {
+      case 0: return launchThermoBatchV<T, 0>(b, maxK, s);
+      case 1: return launchThermoBatchV<T, 1>(b, maxK, s);
+      case 4: return launchThermoBatchV<T, 4>(b, maxK, s);
+      case 5: return launchThermoBatchV<T, 5>(b, maxK, s);
+      case 8: return launchThermoBatchV<T, 8>(b, maxK, s);
+      case 9: return launchThermoBatchV<T, 9>(b, maxK, s);
+      case 12: return launchThermoBatchV<T, 12>(b, maxK, s);
+      case 13: return launchThermoBatchV<T, 13>(b, maxK, s);
+      default: setError("thermoBatch: bad variant %d", variant); return MKF_ERR_ARG;
+   }
+}
+
+int launchThermoGroups(const FieldTask *dTasks, const BatchChunk *dChunks, const std::vector<ThermoGroup> &groups,
+                       unsigned *counters, int enc, cudaStream_t s)
+{
+   int rc = MKF_OK;
+   for (const ThermoGroup &g : groups) {
+      if (rc != MKF_OK) { break; }
+      if (g.maxK < 1 || g.maxK > MKF_MAX_THRESH) { setError("thermoBatch: bad threshold count %d", g.maxK); return MKF_ERR_ARG; }
+      BatchArgs b;
+      b.tasks = dTasks;
+      b.chunks = dChunks + g.c0;
+      b.nChunks = g.c1 - g.c0;
+      b.counter = counters + g.variant;
+      rc = enc == ENC_F32 ? launchThermoBatchT<float>(b, g.variant, g.maxK, s)
+                          : launchThermoBatchT<double>(b, g.variant, g.maxK, s);
+   }
+   return rc;
 }
 
 template <typename T, bool GE>
