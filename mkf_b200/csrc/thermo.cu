@@ -305,7 +305,8 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
    const int xl = INNER ? x0 + lane : min(x0 + lane, a.X - 1);  // clamped: lanes past the row end re-read it
    const int lastRow = a.Y - 1 - y0;                              // clamped: rows past it re-read it
    const int jlo = ys - y0, jhi = ye - y0;                        // counted row pairs j in [jlo, jhi)
-   const uint32_t vx = (x0 + lane >= xs && x0 + lane < xe) ? 0xFFFFFFFFu : 0u;
+   const bool laneIn = x0 + lane >= xs && x0 + lane < xe;
+   const uint32_t vx = laneIn ? 0xFFFFFFFFu : 0u;
    const long long rowStep = (long long)W * a.sy, planeStep = (long long)W * a.sz;
    const uint32_t rowBytes = (uint32_t)(rowStep * 4);
    const long long e00 = (long long)xl * a.sx + (long long)y0 * a.sy + (long long)z0 * a.sz;
@@ -389,9 +390,16 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
          const uint32_t fc = __byte_perm(ePrev, e, 0x5410);
          const uint32_t fmn = min(mnPrev, mn), fmx = max(mxPrev, mx);
          const uint32_t rmin = min(sM[j] & 0xFFu, fmn);
-         const uint32_t vmask = (j >= jlo && j < jhi) ? vx : 0u;
-         const uint32_t rmax = vmask ? max(sM[j] >> 8, fmx) : rmin;  // uncounted cells: no mixed codes
-         ones.add(j, thermo(rmin) & vmask);
+         uint32_t rmax;  // uncounted cells: rmax = rmin, no mixed codes
+         if (W == 2) {   // (measured: a predicate is faster for FP64 fields, a lane mask for FP32)
+            const bool counted = j >= jlo && j < jhi && laneIn;
+            rmax = counted ? max(sM[j] >> 8, fmx) : rmin;
+            ones.add(j, counted ? thermo(rmin) : 0u);
+         } else {
+            const uint32_t vmask = (j >= jlo && j < jhi) ? vx : 0u;
+            rmax = vmask ? max(sM[j] >> 8, fmx) : rmin;
+            ones.add(j, thermo(rmin) & vmask);
+         }
          {
             // Mixed codes, k = rmin .. rmax - 1. With d = corner rank - rmin per byte, the code
             // for k = rmin + q marks the corners with d > q; with b0, b1 the masks of corners
@@ -421,7 +429,7 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
             }
          }
          sF[j] = fc;
-         sM[j] = fmn | (fmx << 8);
+         sM[j] = W == 2 ? fmx * 256u + fmn : fmn | (fmx << 8);
          ePrev = e;
          mnPrev = mn;
          mxPrev = mx;
