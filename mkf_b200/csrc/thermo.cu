@@ -138,10 +138,15 @@ struct PlaneOnes
 
 // Shared state of a CTA while it counts one field: the rank table, the thresholds, and the
 // per-threshold totals. The [K][256] histogram and the warps' staging planes are dynamic.
+// Rank-table value of the buckets whose keys need the exact slow path on FP64 fields (infinities
+// and NaNs, and magnitudes below 2^-1022 whose high word alone may not order them): above every
+// rank, so one compare finds them. On FP32 fields these buckets hold only NaN keys.
+static constexpr uint32_t kSlowBucket = MKF_MAX_THRESH + 1;
+static constexpr int kThKeys = MKF_MAX_THRESH + 8;  // keys indexed up to kSlowBucket + 3
 struct ThermoShared
 {
    alignas(16) uint8_t lut[kLutSize];
-   uint32_t key[MKF_MAX_THRESH + 4];  // padded: a bucket's candidates may run past the last key
+   uint32_t key[kThKeys];  // padded: a bucket's candidates may run past the last key (or the sentinel)
    double tlo[64];
    double thi[64];
    uint32_t ones[MKF_MAX_THRESH];
@@ -178,7 +183,7 @@ __device__ void ctaSetup(const P &a, ThermoShared &S, uint32_t *hist)
       S.tlo[i] = a.tlo[i];
       S.thi[i] = a.thi[i];
    }
-   for (int i = threadIdx.x; i < MKF_MAX_THRESH + 4; i += blockDim.x) { S.key[i] = (i < K) ? a.tkey[i] : 0xFFFFFFFFu; }
+   for (int i = threadIdx.x; i < kThKeys; i += blockDim.x) { S.key[i] = (i < K) ? a.tkey[i] : 0xFFFFFFFFu; }
    __syncthreads();
    // bucket b -> number of threshold keys below the bucket's first key (keys sorted: binary
    // search), four buckets per 32-bit store
@@ -193,7 +198,8 @@ __device__ void ctaSetup(const P &a, ThermoShared &S, uint32_t *hist)
             const int mid = (lo + hi) >> 1;
             if (S.key[mid] < start) { lo = mid + 1; } else { hi = mid; }
          }
-         word |= (uint32_t)lo << (8 * q);
+         const uint32_t b = 4 * w + q;  // keys < 0x00100000 or >= 0xFFF00000
+         word |= (b < 4 || b >= kLutSize - 4 ? kSlowBucket : (uint32_t)lo) << (8 * q);
       }
       lut4[w] = word;
    }
@@ -325,7 +331,7 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
    };
    loadPlane(Pz);
 
-   uint32_t sF[TY], sM[TY];  // previous plane: face ranks, min | max << 8 per row pair
+   uint32_t sF[TY], sM[TY];  // previous plane: face ranks, max * 65536 + min per row pair
    PlaneOnes<TY> ones;
    for (int p = 0; p <= nPln; ++p) {
       uint32_t r[TY + 1];
@@ -350,7 +356,7 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
             tie = tie || key == cc;
          }
          if (W == 2) {
-            slow = slow || tie || key >= 0xFFF00000u || key < 0x00100000u;
+            slow = slow || tie || r0 >= kSlowBucket;
          } else {
             r[j] = ((wj & 0x7FFFFFFFu) > 0x7F800000u) ? nanRank : r[j];
          }
@@ -373,7 +379,7 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
             const uint32_t e = __byte_perm(r[j + 1], rR, 0x0040);
             const uint32_t mn = min(r[j + 1], rR), mx = max(r[j + 1], rR);
             sF[j] = __byte_perm(ePrev, e, 0x5410);
-            sM[j] = min(mnPrev, mn) | (max(mxPrev, mx) << 8);
+            sM[j] = max(mxPrev, mx) * 65536u + min(mnPrev, mn);
             ePrev = e;
             mnPrev = mn;
             mxPrev = mx;
@@ -389,15 +395,17 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
          const uint32_t mn = min(r[j + 1], rR), mx = max(r[j + 1], rR);
          const uint32_t fc = __byte_perm(ePrev, e, 0x5410);
          const uint32_t fmn = min(mnPrev, mn), fmx = max(mxPrev, mx);
-         const uint32_t rmin = min(sM[j] & 0xFFu, fmn);
+         // previous face: max * 65536 + min, unpacked by multiplies (FMA pipe, not the ALU's)
+         const uint32_t pmx = __umulhi(sM[j], 65536u), pmn = sM[j] - pmx * 65536u;
+         const uint32_t rmin = min(pmn, fmn);
          uint32_t rmax;  // uncounted cells: rmax = rmin, no mixed codes
          if (W == 2) {   // (measured: a predicate is faster for FP64 fields, a lane mask for FP32)
             const bool counted = j >= jlo && j < jhi && laneIn;
-            rmax = counted ? max(sM[j] >> 8, fmx) : rmin;
+            rmax = counted ? max(pmx, fmx) : rmin;
             ones.add(j, counted ? thermo(rmin) : 0u);
          } else {
             const uint32_t vmask = (j >= jlo && j < jhi) ? vx : 0u;
-            rmax = vmask ? max(sM[j] >> 8, fmx) : rmin;
+            rmax = vmask ? max(pmx, fmx) : rmin;
             ones.add(j, thermo(rmin) & vmask);
          }
          {
@@ -407,7 +415,8 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
             // b1, b0 & b1. Wider cells (1 in 100 on a unit-variance field with thresholds 0.27
             // apart) are queued and counted after the row loop.
             const uint32_t R0 = sF[j], R1 = fc;
-            const uint32_t spread = rmax - rmin;
+            uint32_t spread;  // rmax - rmin as a multiply-add (FMA pipe)
+            asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(spread) : "r"(rmin), "r"(0xFFFFFFFFu), "r"(rmax));
             const uint32_t rowAddr = hist32 + rmin * (kHistRow * 4);
             // integer multiply-adds (not shifts and logic) where they serve: the kernel is bound by
             // the integer ALU pipe, and these run on the FMA pipe
@@ -429,7 +438,7 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
             }
          }
          sF[j] = fc;
-         sM[j] = W == 2 ? fmx * 256u + fmn : fmn | (fmx << 8);
+         sM[j] = fmx * 65536u + fmn;
          ePrev = e;
          mnPrev = mn;
          mxPrev = mx;
