@@ -619,3 +619,25 @@ def test_dense_thresholds_on_a_smooth_field(mkf, oracle, cuda, dtype):
     plan = mkf.BatchPlan([fd, fd], ths)
     assert (u64(plan.launch()) == np.concatenate(want)).all()
     plan.close()
+
+
+def test_batch_plan_every_rank_table_variant(mkf, oracle, cuda):
+    """One plan holding every variant of the batched rank-table kernel (FP32 / FP64 x relation
+    > / >= x thresholds alone or sharing rank-table buckets x whole or edge-shifted tiles), which a
+    launch runs as one kernel per variant over its group of chunks; against the oracle."""
+    rng = np.random.default_rng(71)
+    spread = [-1.2, -0.7, -0.3, 0.0, 0.2, 0.6, 0.9, 1.4]
+    paired = [-0.3, -0.3001, 0.1, 0.1001, 0.5, 0.5001, 1.0, 1.0001]  # pairs share a bucket
+    fields, ths, masks, want = [], [], [], []
+    for dt in (np.float32, np.float64):
+        for m in (mkf.BMC_GT, mkf.BMC_GT | mkf.BMC_EQ):
+            for t in (spread, paired):
+                for shape in ((30, 40, 45), (24, 20, 19)):  # X, Y >= 32: shifted tiles; else plain
+                    f = rng.standard_normal(shape).astype(dt)
+                    Z, Y, X = shape
+                    want.append(oracle.bpfd_field(f, (X, Y, Z), t, m))
+                    fields.append(to_dev(f, cuda)); ths.append(t); masks.append(m)
+    plan = mkf.BatchPlan(fields, ths, masks)
+    assert (u64(plan.launch()) == np.concatenate(want)).all()
+    assert (u64(plan.launch_graph()) == np.concatenate(want)).all()
+    plan.close()
