@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 #include "fused.cuh"
 
@@ -127,11 +128,63 @@ struct PlaneOnes
       fa(eights, c16, eights, p8, c8);
       ripple(c16);
    }
+   // the interface of the paired tree below (plane parity unused here)
+   __device__ __forceinline__ void add(const int J, uint32_t w, bool) { add(J, w); }
+   __device__ __forceinline__ void finish() {}
    __device__ __forceinline__ uint32_t total(int k) const
    {
       uint32_t v = ((ones >> k) & 1u) + 2u * ((twos >> k) & 1u) + 4u * ((fours >> k) & 1u) + 8u * ((eights >> k) & 1u);
 #pragma unroll
       for (int i = 0; i < 8; i++) { v += ((uint32_t)NROW << i) * ((hi[i] >> k) & 1u); }
+      return v;
+   }
+};
+
+// The 8-row tree with the weight-8 carries of two planes combined before they ripple: the top
+// carry of an even plane waits in p8, the odd plane's joins it in the eights slice, and only
+// the weight-16 carry ripples into hi[] (16 << i each), once per two planes. finish() folds a
+// carry still waiting after the last plane.
+struct PlaneOnesPaired
+{
+   uint32_t ones = 0, twos = 0, fours = 0, eights = 0;
+   uint32_t hi[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // 255 planes x 8 rows = 2040 < 16 x 256
+   uint32_t p1 = 0, p2 = 0, p4 = 0, p8 = 0;
+   __device__ __forceinline__ void ripple(uint32_t c)
+   {
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+         const uint32_t t = hi[i] & c;
+         hi[i] ^= c;
+         c = t;
+      }
+   }
+   // J is the row index (compile-time in the unrolled row loop); odd: this plane closes a pair
+   __device__ __forceinline__ void add(const int J, uint32_t w, bool odd)
+   {
+      if ((J & 1) == 0) { p1 = w; return; }
+      uint32_t c2, c4, c8, c16;
+      PlaneOnes<8>::fa(ones, c2, ones, p1, w);
+      if ((J & 2) == 0) { p2 = c2; return; }
+      PlaneOnes<8>::fa(twos, c4, twos, p2, c2);
+      if ((J & 4) == 0) { p4 = c4; return; }
+      PlaneOnes<8>::fa(fours, c8, fours, p4, c4);
+      if (!odd) { p8 = c8; return; }
+      PlaneOnes<8>::fa(eights, c16, eights, p8, c8);
+      p8 = 0;
+      ripple(c16);
+   }
+   __device__ __forceinline__ void finish()
+   {
+      const uint32_t c16 = eights & p8;
+      eights ^= p8;
+      p8 = 0;
+      ripple(c16);
+   }
+   __device__ __forceinline__ uint32_t total(int k) const
+   {
+      uint32_t v = ((ones >> k) & 1u) + 2u * ((twos >> k) & 1u) + 4u * ((fours >> k) & 1u) + 8u * ((eights >> k) & 1u);
+#pragma unroll
+      for (int i = 0; i < 8; i++) { v += (16u << i) * ((hi[i] >> k) & 1u); }
       return v;
    }
 };
@@ -312,6 +365,8 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
    const int lastRow = a.Y - 1 - y0;                              // clamped: rows past it re-read it
    const int jlo = ys - y0, jhi = ye - y0;                        // counted row pairs j in [jlo, jhi)
    const bool laneIn = x0 + lane >= xs && x0 + lane < xe;
+   // bit j: row pair j of this lane is counted
+   const uint32_t rowsOK = laneIn ? ((1u << jhi) - 1u) & ~((1u << jlo) - 1u) : 0u;
    const uint32_t vx = laneIn ? 0xFFFFFFFFu : 0u;
    const long long rowStep = (long long)W * a.sy, planeStep = (long long)W * a.sz;
    const uint32_t rowBytes = (uint32_t)(rowStep * 4);
@@ -332,7 +387,7 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
    loadPlane(Pz);
 
    uint32_t sF[TY], sM[TY];  // previous plane: face ranks, max * 65536 + min per row pair
-   PlaneOnes<TY> ones;
+   typename std::conditional<TY == 8, PlaneOnesPaired, PlaneOnes<TY>>::type ones;
    for (int p = 0; p <= nPln; ++p) {
       uint32_t r[TY + 1];
 #pragma unroll
@@ -386,6 +441,7 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
          }
          continue;
       }
+      const bool oddPlane = (p & 1) == 0;  // counted planes 1, 2 | 3, 4 | ...: this one closes a pair
       uint4 wq[TY];  // cells of this plane spanning more than 3 thresholds (about 1 in 100)
       int nwq = 0;
 #pragma unroll
@@ -400,13 +456,13 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
          const uint32_t rmin = min(pmn, fmn);
          uint32_t rmax;  // uncounted cells: rmax = rmin, no mixed codes
          if (W == 2) {   // (measured: a predicate is faster for FP64 fields, a lane mask for FP32)
-            const bool counted = j >= jlo && j < jhi && laneIn;
+            const bool counted = (rowsOK & (1u << j)) != 0;
             rmax = counted ? max(pmx, fmx) : rmin;
-            ones.add(j, counted ? thermo(rmin) : 0u);
+            ones.add(j, counted ? thermo(rmin) : 0u, oddPlane);
          } else {
-            const uint32_t vmask = (j >= jlo && j < jhi) ? vx : 0u;
+            const uint32_t vmask = (rowsOK & (1u << j)) ? 0xFFFFFFFFu : 0u;
             rmax = vmask ? max(pmx, fmx) : rmin;
-            ones.add(j, thermo(rmin) & vmask);
+            ones.add(j, thermo(rmin) & vmask, oddPlane);
          }
          {
             // Mixed codes, k = rmin .. rmax - 1. With d = corner rank - rmin per byte, the code
@@ -472,6 +528,7 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
          }
       }
    }
+   ones.finish();
    for (int k = 0; k < K; ++k) {
       const uint32_t s = __reduce_add_sync(FULL, ones.total(k));
       if (lane == 0 && s) { atomicAdd(&S.ones[k], s); }
