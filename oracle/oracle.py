@@ -1,7 +1,7 @@
 """ctypes access to the CPU oracles. TEST INFRASTRUCTURE ONLY.
 
-Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` may import
-this module; the product library never does.
+Only the tests, ``__graft_entry__.smoke()``, and the CPU-baseline leg and the reference arm
+(``--impl reference``) of ``bench.py`` may import this module; the product library never does.
 
 * :class:`Oracle` wraps ``liboracle.so``, the project's CPU restatement of the MKF path
   (``mkf_oracle.c``).
