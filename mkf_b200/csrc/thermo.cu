@@ -191,9 +191,10 @@ struct PlaneOnesPaired
 
 // Shared state of a CTA while it counts one field: the rank table, the thresholds, and the
 // per-threshold totals. The [K][256] histogram and the warps' staging planes are dynamic.
-// Rank-table value of the buckets whose keys need the exact slow path on FP64 fields (infinities
-// and NaNs, and magnitudes below 2^-1022 whose high word alone may not order them): above every
-// rank, so one compare finds them. On FP32 fields these buckets hold only NaN keys.
+// Rank-table value of the buckets whose keys take the exact slow path: above every rank, so one
+// compare finds them. They are the keys below 0x00800000 and from 0xFF800000 up: the infinities
+// and NaNs of FP32 fields, and of FP64 fields (ranked by the high word) the infinities, NaNs and
+// magnitudes of 2^1017 and more.
 static constexpr uint32_t kSlowBucket = MKF_MAX_THRESH + 1;
 static constexpr int kThKeys = MKF_MAX_THRESH + 8;  // keys indexed up to kSlowBucket + 3
 struct ThermoShared
@@ -251,8 +252,8 @@ __device__ void ctaSetup(const P &a, ThermoShared &S, uint32_t *hist)
             const int mid = (lo + hi) >> 1;
             if (S.key[mid] < start) { lo = mid + 1; } else { hi = mid; }
          }
-         const uint32_t b = 4 * w + q;  // keys < 0x00100000 or >= 0xFFF00000
-         word |= (b < 4 || b >= kLutSize - 4 ? kSlowBucket : (uint32_t)lo) << (8 * q);
+         const uint32_t b = 4 * w + q;  // keys < 0x00800000 or >= 0xFF800000
+         word |= (b < 32 || b >= kLutSize - 32 ? kSlowBucket : (uint32_t)lo) << (8 * q);
       }
       lut4[w] = word;
    }
@@ -410,13 +411,10 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
             r[j] += GE ? (key >= cc) : (key > cc);
             tie = tie || key == cc;
          }
-         if (W == 2) {
-            slow = slow || tie || r0 >= kSlowBucket;
-         } else {
-            r[j] = ((wj & 0x7FFFFFFFu) > 0x7F800000u) ? nanRank : r[j];
-         }
+         // FP64: a high word equal to a threshold's needs the low word too
+         slow = slow || (W == 2 && tie) || r0 >= kSlowBucket;
       }
-      if (W == 2 && slow) {
+      if (slow) {
          const T *Fe = reinterpret_cast<const T *>(a.f);
          const long long e0 = e00 + (long long)p * a.sz;
 #pragma unroll

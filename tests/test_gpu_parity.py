@@ -641,3 +641,26 @@ def test_batch_plan_every_rank_table_variant(mkf, oracle, cuda):
     assert (u64(plan.launch()) == np.concatenate(want)).all()
     assert (u64(plan.launch_graph()) == np.concatenate(want)).all()
     plan.close()
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_rank_table_special_values_in_the_field(mkf, oracle, cuda, dtype):
+    """NaN, +-inf and (FP64) magnitudes near the top of the range sprinkled into a field counted
+    by the rank-table kernel (16 ordinary thresholds, whole tiles): those elements take the exact
+    rank path, every relation of one kind, against the oracle."""
+    rng = np.random.default_rng(83)
+    f = rng.standard_normal((30, 48, 70))
+    flat = f.ravel()
+    idx = rng.choice(flat.size, 3000, replace=False)
+    flat[idx[:600]] = np.nan
+    flat[idx[600:1200]] = np.inf
+    flat[idx[1200:1800]] = -np.inf
+    if dtype == np.float64:
+        flat[idx[1800:2400]] = 1e308
+        flat[idx[2400:]] = -3e307
+    f = f.astype(dtype)
+    Z, Y, X = f.shape
+    t = np.linspace(-2, 2, 16)
+    for mask in (mkf.BMC_GT, mkf.BMC_GT | mkf.BMC_EQ, mkf.BMC_LT, mkf.BMC_LT | mkf.BMC_EQ):
+        got = u64(mkf.field_bpfd(to_dev(f, cuda), t, mask))
+        assert (got == oracle.bpfd_field(f, (X, Y, Z), t, [mask] * len(t))).all(), mask
