@@ -664,3 +664,19 @@ def test_rank_table_special_values_in_the_field(mkf, oracle, cuda, dtype):
     for mask in (mkf.BMC_GT, mkf.BMC_GT | mkf.BMC_EQ, mkf.BMC_LT, mkf.BMC_LT | mkf.BMC_EQ):
         got = u64(mkf.field_bpfd(to_dev(f, cuda), t, mask))
         assert (got == oracle.bpfd_field(f, (X, Y, Z), t, [mask] * len(t))).all(), mask
+
+
+@pytest.mark.parametrize("prof_id", [1, 2, 3])
+def test_dropin_two_plane_buffer_profile(mkf, oracle, cuda, prof_id):
+    """A profile with a nonzero low nibble selects the reference's small buffer layout (setBMO,
+    binMapUtil.c:60-87: two rows, two planes). The drop-in maps exactly that window of the field
+    (rows 0-1 of planes 0-1) and counts its one row pair of one plane pair; the reference maps the
+    whole field into the small buffer there (binMapCUDA.cu:167-199), past its end."""
+    rng = np.random.default_rng(90 + prof_id)
+    f = rng.standard_normal((7, 9, 70)).astype(np.float32)
+    fd = to_dev(f, cuda)
+    pbm, org, _ = mkf.bin_map_cuda(fd, ">", 0.25, prof_id=prof_id)
+    assert (org.rowPairs, org.planePairs) == (1, 1)
+    got = u64(mkf.get_bpfd(pbm, org))
+    sub = np.ascontiguousarray(f[:2, :2, :])
+    assert (got == oracle.bpfd_field(sub, (70, 2, 2), [0.25], mkf.BMC_GT)[0]).all()
