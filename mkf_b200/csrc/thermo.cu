@@ -423,15 +423,16 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
          }
       }
       uint32_t rR = __shfl_down_sync(FULL, r[0], 1);
-      uint32_t ePrev = __byte_perm(r[0], rR, 0x0040);
+      // faces as multiply-adds (ranks < 256): e = r | rR << 8, face = e(row j) | e(row j + 1) << 16
+      uint32_t ePrev = rR * 256u + r[0];
       uint32_t mnPrev = min(r[0], rR), mxPrev = max(r[0], rR);
       if (p == 0) {
 #pragma unroll
          for (int j = 0; j < TY; ++j) {
             rR = __shfl_down_sync(FULL, r[j + 1], 1);
-            const uint32_t e = __byte_perm(r[j + 1], rR, 0x0040);
+            const uint32_t e = rR * 256u + r[j + 1];
             const uint32_t mn = min(r[j + 1], rR), mx = max(r[j + 1], rR);
-            sF[j] = __byte_perm(ePrev, e, 0x5410);
+            sF[j] = e * 65536u + ePrev;
             sM[j] = max(mxPrev, mx) * 65536u + min(mnPrev, mn);
             ePrev = e;
             mnPrev = mn;
@@ -445,9 +446,9 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
 #pragma unroll
       for (int j = 0; j < TY; ++j) {
          rR = __shfl_down_sync(FULL, r[j + 1], 1);
-         const uint32_t e = __byte_perm(r[j + 1], rR, 0x0040);
+         const uint32_t e = rR * 256u + r[j + 1];
          const uint32_t mn = min(r[j + 1], rR), mx = max(r[j + 1], rR);
-         const uint32_t fc = __byte_perm(ePrev, e, 0x5410);
+         const uint32_t fc = e * 65536u + ePrev;
          const uint32_t fmn = min(mnPrev, mn), fmx = max(mxPrev, mx);
          // previous face: max * 65536 + min, unpacked by multiplies (FMA pipe, not the ALU's)
          const uint32_t pmx = __umulhi(sM[j], 65536u), pmn = sM[j] - pmx * 65536u;
