@@ -3,22 +3,26 @@
 // Sorted thresholds make an element's K map bits a thermometer, bits[k] = (k < rank), so an
 // element reduces to one rank 0..K. The rank is found with a table over order-preserving 32-bit
 // keys: key(f) orders like f, the table maps key >> 18 (16384 buckets) to the number of
-// threshold keys below the bucket, and one compare with the bucket's only candidate threshold
-// finishes the count. FP32 keys are exact. A FP64 element is read as its high word only (same
-// DRAM sectors, half the load bandwidth into the SM); when that word ties with the candidate's or
-// the element is inf/NaN, the element is re-read whole and ranked exactly by binary search.
+// threshold keys below the bucket, and one compare with the bucket's candidate threshold (up to
+// four when thresholds share a bucket) finishes the count. FP32 keys are exact. A FP64 element is
+// read as its high word only (same DRAM sectors, half the load bandwidth into the SM); when that
+// word ties with the candidate's, the element is re-read whole and ranked exactly by binary
+// search. Infinities and NaNs (and FP64 magnitudes of 2^1017 and more) fall in table buckets
+// flagged for the same exact path.
 //
 // A warp owns 32 x positions (31 cells, neighbouring columns overlap by one element), TY row pairs
 // (TY + 1 rows) and D planes; it walks the planes, loading the next plane's TY + 1 words per lane
 // into registers while the current one is ranked and counted, and keeping per row pair of the
-// previous plane the four corner ranks (one byte each) and their min | max << 8. Work items at the
-// field's +x / +y edge are shifted back inside the field (their cells already owned by the
+// previous plane the four corner ranks (one byte each) and their max * 65536 + min. Work items at
+// the field's +x / +y edge are shifted back inside the field (their cells already owned by the
 // neighbouring item are masked), so no load needs a clamp. A cell's pattern for threshold k is
-// all-ones for k < min rank, all-zeros for k >= max rank, and is formed with byte arithmetic on
-// the two faces' packed ranks only for k in between: three predicated slots cover almost every
-// cell, a loop the rest. Codes go to the per-CTA [K][256] shared histogram. All-ones counts are
-// summed per threshold with bit-sliced carry-save adders and all-zeros counts follow from the
-// number of cells, as in fused.cu.
+// all-ones for k < min rank, all-zeros for k >= max rank, and is formed from the two faces'
+// packed ranks only for k in between: three unpredicated atomic slots cover the cells spanning up
+// to 3 thresholds (99 % on a smooth field); wider cells are queued and counted after the row loop.
+// Codes go to the per-CTA [K][256] shared histogram. All-ones counts are summed per threshold with
+// bit-sliced carry-save adders and all-zeros counts follow from the number of cells, as in
+// fused.cu. The kernel is bound by the integer ALU pipe, so arithmetic that can be a multiply-add
+// is written as one (it runs on the FMA pipe).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
