@@ -10,12 +10,13 @@ Inputs are 8.6 GB, far larger than the 126 MB L2, so no flush is needed between 
   e2e       Gvoxel/s through the host-buffer entry point mkfFieldBPFDHost: each step copies the
             pinned host field to the GPU (slabs overlapped with counting) and the counts back
   roofline  the fused kernel's algorithmic bytes / its CUDA-event time vs measured HBM peak
-  cpu_baseline  the reference MKF C path (compiled from its sources) on this host's cores, on a
-            bounded slab sample of the same kind of field
+  cpu_baseline  the reference MKF C path (compiled from its sources) on this host's cores over the
+            whole field; its counts must equal the timed counts (counts_equal_reference); beside
+            it the reference's single-thread entry point on a 16-plane slab
 
 With torchrun (N > 1) every rank counts its own 1024^3 slab (1025 planes: one halo plane) of a
-field sharded along z and the 16 x 256 partial counts are summed with an NCCL all-reduce each
-step (weak scaling). `--impl reference` times the reference C path alone (rank 0) and, as a
+field sharded along z through mkf_b200.shard.sharded_field_bpfd, which sums the 16 x 256 partial
+counts with an NCCL all-reduce each step (weak scaling). `--impl reference` times the reference C path alone (rank 0) and, as a
 second reference point under "reference_cuda", the reference's own CUDA path compiled for sm_100a.
 """
 from __future__ import annotations
@@ -454,11 +455,12 @@ def plane_wave_field(out, n_waves, seed, step, chunk=16):
     torch.cuda.synchronize(dev)
 
 
-def run_insitu_workload(dev, steps=3, shape=(1536, 2048, 2048), seed=SEED + 6):
-    """The large in-situ series (2048 x 2048 x 1536 FP32, 25.8 GB; 3 of its 20 time steps), thresholds
-    {-0.5, 0, 0.5}: each step counted device-resident (the field in HBM; CUDA events) and streamed
-    from pinned host memory through mkfFieldBPFDHost (wall clock, host -> device copies overlapped
-    with counting); the two give the same counts."""
+def run_insitu_workload(dev, steps=20, streamed_steps=3, shape=(1536, 2048, 2048), seed=SEED + 6):
+    """The large in-situ series (2048 x 2048 x 1536 FP32, 25.8 GB), thresholds {-0.5, 0, 0.5}: all
+    20 time steps counted device-resident (the field in HBM, refilled by the generator each step;
+    CUDA events around the count), and the first `streamed_steps` of them also streamed from pinned
+    host memory through mkfFieldBPFDHost (wall clock, host -> device copies overlapped with
+    counting: about 0.5 s of PCIe per step, so not every step), with the same counts."""
     import torch
 
     import mkf_b200
@@ -469,26 +471,33 @@ def run_insitu_workload(dev, steps=3, shape=(1536, 2048, 2048), seed=SEED + 6):
     vox = f.numel()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     dev_ms, host_s, same = [], [], True
+    out = None
     for step in range(steps):
         plane_wave_field(f, 256, seed, step)
-        out = mkf_b200.field_bpfd(f, t, mkf_b200.BMC_GT)  # warm-up
+        if out is None:
+            out = mkf_b200.field_bpfd(f, t, mkf_b200.BMC_GT)  # warm-up
+        out.zero_()
         e0.record()
-        out = mkf_b200.field_bpfd(f, t, mkf_b200.BMC_GT, out=out)
+        mkf_b200.field_bpfd(f, t, mkf_b200.BMC_GT, out=out)
         e1.record()
         torch.cuda.synchronize(dev)
         dev_ms.append(e0.elapsed_time(e1))
-        h.copy_(f)
-        t0 = time.perf_counter()
-        hc = mkf_b200.field_bpfd_host(h.numpy(), t, mkf_b200.BMC_GT)
-        host_s.append(time.perf_counter() - t0)
-        same = same and bool((hc == out.cpu().numpy().view(np.uint64)).all())
+        if step < streamed_steps:
+            h.copy_(f)
+            t0 = time.perf_counter()
+            hc = mkf_b200.field_bpfd_host(h.numpy(), t, mkf_b200.BMC_GT)
+            host_s.append(time.perf_counter() - t0)
+            same = same and bool((hc == out.cpu().numpy().view(np.uint64)).all())
     del f, h
     torch.cuda.empty_cache()
     return {
-        "workload": "2048 x 2048 x 1536 FP32 plane-wave series, 256 waves, thresholds {-0.5, 0, 0.5}, "
-                    f"{steps} time steps",
+        "workload": "2048 x 2048 x 1536 FP32 plane-wave series, 256 waves, thresholds {-0.5, 0, 0.5}",
+        "steps_device_resident": steps,
+        "steps_streamed": streamed_steps,
         "device_resident_ms_per_step": float(np.mean(dev_ms)),
+        "device_resident_ms_per_step_min_max": [float(np.min(dev_ms)), float(np.max(dev_ms))],
         "device_resident_gvoxel_per_s": vox / (np.mean(dev_ms) * 1e-3) * 1e-9,
+        "device_resident_gb_per_s": vox * 4 / (np.mean(dev_ms) * 1e-3) * 1e-9,
         "streamed_s_per_step": float(np.mean(host_s)),
         "streamed_gvoxel_per_s": vox / np.mean(host_s) * 1e-9,
         "streamed_h2d_gb_per_s": vox * 4 / np.mean(host_s) * 1e-9,
@@ -636,14 +645,44 @@ def calibrate_planes(f: np.ndarray, threads: int, target_s: float, max_planes: i
     return int(max(2, min(max_planes, (target_s - fixed) / per_plane)))
 
 
-def cpu_baseline(f: np.ndarray, target_s: float = 10.0):
-    """The reference C path on this host's cores, on a slab of the benchmark field itself."""
+def cpu_baseline(f: np.ndarray, counts: np.ndarray | None = None, target_s: float = 10.0):
+    """The reference C path on this host's cores over the whole benchmark field (all 1023 plane
+    pairs, one reference call per threshold, each split into z-slabs over every host thread), its
+    counts compared with `counts` (the GPU's, uint64 [16, 256]) bin by bin as the reference's own
+    test compares its CPU and GPU distributions (mkfTest.c:64-85); plus the reference's
+    single-thread entry point exactly as written (mkfAccGetBPFDSimple, mkfACC.c:206-239) on a
+    16-plane slab. Without the reference build, the project's port on a calibrated slab."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    from oracle import RefOracle
+
     threads = cpu_threads()
-    planes = calibrate_planes(f, threads, target_s, N_SIDE - 1)
-    dt, vox, kind, thr = reference_sample(f, planes, threads)
-    return {"value": vox / dt * 1e-9, "unit": "Gvoxel/s", "cores": thr, "kind": kind,
-            "sample": f"{planes} plane pairs of the 1024^3 FP64 benchmark field, 16 thresholds "
-                      f"(16 reference calls), {dt:.2f} s"}
+    if not RefOracle.available():
+        planes = calibrate_planes(f, threads, target_s, N_SIDE - 1)
+        dt, vox, kind, thr = reference_sample(f, planes, threads)
+        return {"value": vox / dt * 1e-9, "unit": "Gvoxel/s", "cores": thr, "kind": kind,
+                "sample": f"{planes} plane pairs of the 1024^3 FP64 benchmark field, 16 thresholds, {dt:.2f} s"}, None
+    ref = RefOracle()
+    d = (N_SIDE, N_SIDE, N_SIDE)
+    t0 = time.perf_counter()
+    want = np.stack([ref.bpfd_mt(f, d, float(t), 4, threads) for t in THRESHOLDS])
+    dt = time.perf_counter() - t0
+    res = {"value": N_SIDE ** 3 / dt * 1e-9, "unit": "Gvoxel/s", "cores": threads, "kind": "reference",
+           "sample": f"the whole 1024^3 FP64 benchmark field (1023 plane pairs), 16 thresholds (16 reference "
+                     f"calls, z-slabs over {threads} threads), {dt:.2f} s"}
+    if counts is not None:
+        res["counts_equal_gpu"] = bool((want == counts).all())
+    # single thread, as written: one mkfAccGetBPFDSimple call per threshold on 16 plane pairs
+    nz = 17
+    slab = np.ascontiguousarray(f[: nz * N_SIDE * N_SIDE]).reshape(nz, N_SIDE, N_SIDE)
+    t0 = time.perf_counter()
+    one = np.stack([ref.bpfd_simple(slab, (N_SIDE, N_SIDE, nz), float(t), 4) for t in THRESHOLDS])
+    dt1 = time.perf_counter() - t0
+    mt = np.stack([ref.bpfd_mt(slab.ravel(), (N_SIDE, N_SIDE, nz), float(t), 4, threads) for t in THRESHOLDS])
+    res["single_thread"] = {"value": (nz - 1) * N_SIDE * N_SIDE / dt1 * 1e-9, "unit": "Gvoxel/s", "cores": 1,
+                            "entry_point": "mkfAccGetBPFDSimple (mkfACC.c:206-239)",
+                            "sample": f"16 plane pairs x 1024 x 1024 of the benchmark field, 16 thresholds, {dt1:.2f} s",
+                            "counts_equal_multithreaded": bool((one == mt).all())}
+    return res, want
 
 
 def ball256_torch(device, seed=11):
@@ -763,11 +802,15 @@ def run_mkf(args, rank, world, local_rank):
     import torch.distributed as dist
 
     import mkf_b200
+    from mkf_b200 import shard
 
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     mkf_b200.lib()
-    nz = N_SIDE if world == 1 else N_SIDE + 1  # with sharding, one halo plane per rank
+    # this rank's z-slab of a field of world x 1024 cell planes: 1024 cell planes plus one halo
+    # plane (weak scaling; each slab is its own seeded GRF, generated on this rank's GPU)
+    z0, z1 = shard.slab_planes(world * N_SIDE + 1, world, rank) if world > 1 else (0, N_SIDE)
+    nz = z1 - z0
     f = grf_torch(nz, N_SIDE, N_SIDE, SEED + rank, dev)
     vox = N_SIDE ** 3  # voxels of the field (or of this rank's slab) per step
     stream = torch.cuda.current_stream(dev)
@@ -776,14 +819,15 @@ def run_mkf(args, rank, world, local_rank):
     ev_k = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
 
     def step(i=None):
-        out.zero_()
-        if i is not None:
-            ev_k[i][0].record(stream)
-        mkf_b200.field_bpfd(f, THRESHOLDS, mkf_b200.BMC_GT, out=out, accumulate=True, stream=stream)
-        if i is not None:
-            ev_k[i][1].record(stream)
-        if world > 1:
-            dist.all_reduce(out)
+        def counter(slab, thresholds, mask, o):  # the counting kernel, bracketed by CUDA events
+            if i is not None:
+                ev_k[i][0].record(stream)
+            mkf_b200.field_bpfd(slab, thresholds, mask, out=o, accumulate=True, stream=stream)
+            if i is not None:
+                ev_k[i][1].record(stream)
+
+        # zero the counts, count this rank's slab, all-reduce the counts over the ranks (N > 1)
+        shard.sharded_field_bpfd(f, THRESHOLDS, mkf_b200.BMC_GT, out=out, stream=stream, counter=counter)
         mkf_b200._lib.check(mkf_b200.lib().mkfMeasuresF64Dev(meas.data_ptr(), out.data_ptr(), K_THRESH,
                                                              stream.cuda_stream), "mkfMeasuresF64Dev")
 
@@ -875,7 +919,11 @@ def run_mkf(args, rank, world, local_rank):
         "clocks": clocks,
     }
     if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(fh_np.reshape(-1))
+        got = out.cpu().numpy().view(np.uint64)
+        cb, _want = cpu_baseline(fh_np.reshape(-1), got)
+        if "counts_equal_gpu" in cb:
+            line["counts_equal_reference"] = cb.pop("counts_equal_gpu")
+        line["cpu_baseline"] = cb
     if world == 1 and not args.no_secondary:
         del fh, fh_np
         line["plain"] = run_plain_workload(dev)
@@ -883,6 +931,8 @@ def run_mkf(args, rank, world, local_rank):
         line["serving"] = run_serving_workload(dev)
         line["insitu"] = run_insitu_workload(dev)
     print(json.dumps(line), flush=True)
+    if line.get("counts_equal_reference") is False:
+        raise SystemExit("the timed counts differ from the reference C path's")
 
 
 def run_profile_case(args):

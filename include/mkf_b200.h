@@ -14,8 +14,9 @@
  *   - Pattern counts are uint64_t[256] per threshold, laid out [threshold][pattern]. The pattern
  *     code of the cell at (x,y,z) has bit i set when corner (x + (i&1), y + ((i>>1)&1),
  *     z + ((i>>2)&1)) maps to 1, as in the original (bpfdCUDA.cuh:45-61).
- *   - Every row of X elements contributes X-1 cells (the original double-counts rows with
- *     X < 32; see the design notes).
+ *   - Every row of X elements contributes X-1 cells. The original counts 2X-1 cells for rows
+ *     with X < 32, its two counting paths differently (bpfdCUDA.cuh:112-116 re-reads the row's
+ *     first word, mkfACC.c:137-150 reads the next row's), so there the counts differ from it.
  */
 #ifndef MKF_B200_H
 #define MKF_B200_H
@@ -93,12 +94,16 @@ int mkfFieldBPFDHost(uint64_t *pBPFDH, const MKFFieldDesc *pF, const MKFThreshSe
  *   Limit: the staging area must hold two planes, so a plane (X * Y elements) may be at most
  *   16 MiB (e.g. 2048 x 1024 FP64, 2048 x 2048 FP32); larger planes return MKF_ERR_NOMEM.
  *   The first call on each device resolves the arrays' device addresses (cudaGetSymbolAddress)
- *   with that device current; make that first call before any stream capture.
+ *   with that device current and keeps them for the life of the process; a cudaDeviceReset
+ *   reloads the module and moves the arrays, so do not call it after a cudaDeviceReset in the
+ *   same process (this library never resets a device).
  *   All calls on a device share the arrays: calls whose work overlaps on the GPU (different
  *   streams, or different host threads) race and give wrong counts. The counts are cleared at
  *   the start of every call; the staging area keeps the last call's data.
- *   Work runs in order on `stream` (NULL = legacy default stream); returns after the counts are
- *   in pBPFDH (host, uint64_t[nT][256]). pF->p is a planar host field. */
+ *   Work runs in order on `stream` (NULL = legacy default stream) and the call waits for it, so
+ *   it must not be called on a stream that is being captured into a CUDA graph. Returns after
+ *   the counts are in pBPFDH (host, uint64_t[nT][256]). pF->p is a planar host field. Kernel
+ *   choice as mkfFieldBPFD's; when every threshold is a constant map no field data is copied. */
 int mkfFieldBPFDHostNoAlloc(uint64_t *pBPFDH, const MKFFieldDesc *pF, const MKFThreshSet *pT, void *stream);
 
 /* ---- many fields, one launch (no original counterpart; the original runs one field per call) ---- */
@@ -184,6 +189,10 @@ int mkfServerDestroy(MKFServer *server);
  * the previous setting. */
 int mkfTune(const MKFFieldDesc *pF, const MKFThreshSet *pT, void *stream);
 int mkfSetTuning(int batchPlans);
+/* Record `depth` (1..255 planes) as the slab depth of fields of this kind, as mkfTune records the
+ * depth it measured best (for instance one measured in an earlier process); depth 0 forgets the
+ * entry. Counts the field once to learn which kernels it takes (synchronous). */
+int mkfTuneSet(const MKFFieldDesc *pF, const MKFThreshSet *pT, int depth, void *stream);
 
 /* ---- measures (closest original: mkfSelectMeasuresBPFD, mkfUtil.c:94) ---- */
 /* For each of nSets distributions (host uint64_t[nSets][256]) write, in double:

@@ -5,6 +5,7 @@
  * padding must stay exactly as the original declares them (x86-64 LP64 layout).
  *
  *   BinMapF64       replaces MKF src/binMapUtil.h:28-32
+ *   BinMapF32       replaces MKF src/binMapUtil.h:35-40
  *   BMOrg           replaces MKF src/binMapUtil.h:52-57
  *   ConstFieldPtr   replaces MKF src/binMapUtil.h:65
  *   BMFieldInfo     replaces MKF src/binMapUtil.h:69-79
@@ -46,6 +47,9 @@ typedef uint8_t NumEnc;
 #define BMC_AL (0x7)
 
 #define BM_NUMT (1)          /* thresholds per BinMapF64 */
+#define BM_TLB (0)           /* index in BinMapF64.t of the threshold compared for '<' */
+#define BM_TUB (0)           /* index in BinMapF64.t of the threshold compared for '>' */
+#define BM_FLAG_T2IVL (1 << 15)
 #define BMCU_FIELD_MAX 4     /* fields summed by one binMapCUDA call */
 #define MKF_BINS (1 << 8)    /* 2x2x2 cell patterns */
 #define CELL8_PATTERNS (1 << 8)
@@ -56,6 +60,14 @@ typedef struct
    double t[BM_NUMT];
    uint32_t m;
 } BinMapF64;
+
+/* Single-precision form of BinMapF64; no entry point of this library takes it, callers of the
+ * original declare it (binMapUtil.h:35-40). */
+typedef struct
+{
+   float t[BM_NUMT];
+   uint32_t m;
+} BinMapF32;
 
 typedef uint32_t BMStride;
 typedef uint32_t BMPackWord;

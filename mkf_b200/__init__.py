@@ -127,12 +127,16 @@ def field_bpfd_moments(field, thresholds, mask=BMC_GT, stream=None):
     return out, mom
 
 
-def tune(field, thresholds, mask=BMC_GT, stream=None) -> None:
+def tune(field, thresholds, mask=BMC_GT, stream=None, depth=None) -> None:
     """mkfTune: time the candidate slab depths on this CUDA field and keep the fastest for fields
-    of the same kind (synchronous; the counts of later calls do not change, only their speed)."""
+    of the same kind (synchronous; the counts of later calls do not change, only their speed).
+    With `depth`, mkfTuneSet: record that depth for such fields instead (0 forgets the entry)."""
     th = _Thresholds(thresholds, mask)
     strides = None if field.is_contiguous() else field.stride()
     d = _field_desc(field.data_ptr(), _enc_of(field), field.shape, strides)
+    if depth is not None:
+        check(lib().mkfTuneSet(C.byref(d), C.byref(th.ts), int(depth), _stream_ptr(stream)), "mkfTuneSet")
+        return
     check(lib().mkfTune(C.byref(d), C.byref(th.ts), _stream_ptr(stream)), "mkfTune")
 
 

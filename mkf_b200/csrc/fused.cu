@@ -305,6 +305,10 @@ int launchFusedPlain(const FusedPlain &q, cudaStream_t s)
    a.gtm = q.gtm; a.eqm = q.eqm; a.ltm = q.ltm; a.nanP = q.eqm;
    a.nanRank = q.nanRank; a.rankHi = q.rankHi; a.complement = q.complement;
    a.out = q.out;
+   // the kernel choice of fieldBPFD: the word-parallel kernel for one or two thresholds, and for a
+   // few of one relation
+   const int wordMaxK = std::min(kWordMaxK, q.enc == ENC_F32 ? 5 : 6);
+   if (q.K <= 2 || (q.thermo && q.K <= wordMaxK)) { return launchWords(a, q.enc, q.mask, s); }
    constexpr int TY = 16;
    a.D = 64;
    a.nSegX = (q.X - 1 + 30) / 31;

@@ -119,6 +119,7 @@ struct FusedPlain
    int K;
    double tlo[MKF_MAX_THRESH], thi[MKF_MAX_THRESH];
    int outRow[MKF_MAX_THRESH];
+   uint32_t mask[MKF_MAX_THRESH];  // relation mask of each (sorted) threshold
    uint32_t gtm, eqm, ltm, nanRank;
    int thermo, rankHi, complement;
    uint64_t *out;

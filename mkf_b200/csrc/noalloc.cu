@@ -136,6 +136,7 @@ MKF_API int mkfFieldBPFDHostNoAlloc(uint64_t *pBPFDH, const MKFFieldDesc *pF, co
       else { q.tlo[k] = q.thi[k] = t; }
       q.outRow[k] = idx[k];
       const uint32_t m = (pT->m ? pT->m[idx[k]] : pT->mAll) & BMC_AL;
+      q.mask[k] = m;
       q.gtm |= ((m >> 2) & 1u) << k;
       q.eqm |= ((m >> 1) & 1u) << k;
       q.ltm |= (m & 1u) << k;
@@ -149,20 +150,19 @@ MKF_API int mkfFieldBPFDHostNoAlloc(uint64_t *pBPFDH, const MKFFieldDesc *pF, co
    }
 
    if (cells > 0) {
-      // slabs of S plane pairs (S+1 planes staged; the last plane is the next slab's first)
+      // slabs of S plane pairs (S+1 planes staged; the last plane is the next slab's first); no
+      // copies at all when every threshold is a constant map
       size_t S = MKF_NOALLOC_STAGE_BYTES / planeBytes - 1;
       if (S > (size_t)Z - 1) { S = (size_t)Z - 1; }
       const char *src = (const char *)pF->p;
-      for (size_t z0 = 0; z0 + 1 < (size_t)Z && rc == MKF_OK; z0 += S) {
+      for (size_t z0 = 0; n > 0 && z0 + 1 < (size_t)Z && rc == MKF_OK; z0 += S) {
          const size_t nPl = std::min(S + 1, (size_t)Z - z0);
          // same stream: this copy starts only after the previous slab's kernel has finished
          e = cudaMemcpyAsync(sc.stage, src + z0 * planeBytes, nPl * planeBytes, cudaMemcpyHostToDevice, s);
          if (e != cudaSuccess) { rc = cudaFail(e, "slab copy"); break; }
-         if (n > 0) {
-            q.f = sc.stage;
-            q.Z = (int)nPl;
-            rc = launchFusedPlain(q, s);
-         }
+         q.f = sc.stage;
+         q.Z = (int)nPl;
+         rc = launchFusedPlain(q, s);
       }
       for (int c = 0; c < nConst && rc == MKF_OK; c++) {
          rc = launchConstBin((uint64_t *)sc.counts, constRow[c], constBin[c], cells, s);

@@ -122,3 +122,31 @@ MKF_API int mkfTune(const MKFFieldDesc *pF, const MKFThreshSet *pT, void *stream
    if (e1) { cudaEventDestroy(e1); }
    return rc;
 }
+
+MKF_API int mkfTuneSet(const MKFFieldDesc *pF, const MKFThreshSet *pT, int depth, void *stream)
+{
+   if (!pF || !pT || pT->nT < 1 || pT->nT > MKF_MAX_THRESH || depth < 0 || depth > 255) {
+      setError("mkfTuneSet: bad argument");
+      return MKF_ERR_ARG;
+   }
+   cudaStream_t s = (cudaStream_t)stream;
+   uint64_t *tmp = nullptr;
+   cudaError_t e = cudaMalloc(&tmp, (size_t)pT->nT * 256 * sizeof(uint64_t));
+   if (e != cudaSuccess) { return cudaFail(e, "mkfTuneSet: set-up"); }
+   // one counting run learns the kinds of launch this field takes
+   std::vector<TuneKey> seen;
+   tForce = depth > 0 ? depth : 4;
+   tSeen = &seen;
+   int rc = fieldBPFD(tmp, pF, pT, 0, s, nullptr);
+   tForce = 0;
+   tSeen = nullptr;
+   if (rc == MKF_OK) { rc = cudaFail(cudaStreamSynchronize(s), "mkfTuneSet: run"); }
+   if (rc == MKF_OK) {
+      std::lock_guard<std::mutex> lk(gTuneMu);
+      for (const TuneKey &k : seen) {
+         if (depth > 0) { gTuned[k] = depth; } else { gTuned.erase(k); }
+      }
+   }
+   cudaFree(tmp);
+   return rc;
+}

@@ -680,3 +680,97 @@ def test_dropin_two_plane_buffer_profile(mkf, oracle, cuda, prof_id):
     got = u64(mkf.get_bpfd(pbm, org))
     sub = np.ascontiguousarray(f[:2, :2, :])
     assert (got == oracle.bpfd_field(sub, (70, 2, 2), [0.25], mkf.BMC_GT)[0]).all()
+
+
+# ---------------------------------------------------------------- drop-in: maps this library did not make
+
+def _org_of(mkf, X, Y, Z):
+    import ctypes as C
+
+    org = mkf.BMOrg()
+    mkf.lib().setBMO(C.byref(org), (C.c_int * 3)(X, Y, Z), bytes([0]))
+    return org
+
+
+def test_dropin_counts_reference_made_maps(mkf, golden, cuda):
+    """mkfCUDAGetBPFDH on the reference's own packed maps (its CPU map, binMapACC.c:43-93, as the
+    golden fixtures hold them): for X % 32 != 0 their padding bits carry the next row's elements
+    (binMapACC.c:86-90), which the count must ignore. Every map counts to the reference's own
+    distribution. (The reference's test main counts a caller-made ENC_U1 pattern the same way,
+    mkfCUDA.cu:326-331.)"""
+    import torch
+
+    n = 0
+    for key in [str(v) for v in golden["names"] if not str(v).startswith("short_")]:
+        Z, Y, X = golden[key + "/field"].shape
+        org = _org_of(mkf, X, Y, Z)
+        for k in range(golden[key + "/pbm"].shape[0]):
+            words = np.ascontiguousarray(golden[key + "/pbm"][k], np.uint32)
+            pbm = torch.from_numpy(words.view(np.int32).copy()).to(cuda)
+            assert (mkf.get_bpfd_host(pbm, org) == golden[key + "/bpfd"][k]).all(), (key, k)
+            n += 1
+    assert n >= 50
+
+
+@pytest.mark.parametrize("seed", range(3))
+def test_dropin_counts_random_maps_with_padding_bits(mkf, oracle, cuda, seed):
+    """Random packed maps, padding bits random too, several row widths: mkfCUDAGetBPFD (device,
+    accumulating) and mkfCUDAGetBPFDH equal the oracle's count of the same words, which reads
+    only each row's X bits; setting every padding bit changes nothing."""
+    import torch
+
+    rng = np.random.default_rng(700 + seed)
+    for X in (32, 33, 63, 64, 96, 100, 257):
+        Y, Z = int(rng.integers(2, 20)), int(rng.integers(2, 12))
+        row, plane = layout((X, Y, Z))
+        words = rng.integers(0, 1 << 32, size=plane * Z, dtype=np.uint64).astype(np.uint32)
+        org = _org_of(mkf, X, Y, Z)
+        want = oracle.bpfd_pbm(words, (X, Y, Z))
+        assert want.sum() == (X - 1) * (Y - 1) * (Z - 1)
+        pbm = torch.from_numpy(words.view(np.int32).copy()).to(cuda)
+        assert (mkf.get_bpfd_host(pbm, org) == want).all(), X
+        acc = mkf.get_bpfd(pbm, org)
+        acc = mkf.get_bpfd(pbm, org, out=acc)
+        assert (u64(acc) == 2 * want).all(), X
+        padded = words | ~valid_bits_mask(X, Y, Z)
+        pbm = torch.from_numpy(padded.view(np.int32).copy()).to(cuda)
+        assert (mkf.get_bpfd_host(pbm, org) == want).all(), X
+
+
+# ---------------------------------------------------------------- the benchmark configuration against the reference
+
+def test_benchmark_config_equals_reference_c_path(mkf, ref_oracle, cuda):
+    """The benchmark's counting pass (1024 x 1024 rows of a FP64 Gaussian random field, sigma 4,
+    16 thresholds linspace(-2, 2, 16), '>') on 300 planes, against the reference's own C path
+    (oracle/_ref: binMapAcc + addPlaneBPFD per z-slab on all host cores, one call per threshold)
+    bit for bit, as the reference's own test compares its CPU and GPU distributions
+    (mkfTest.c:64-85). Slab depths: the untuned default, the depth the benchmark's tuning keeps on
+    the 1024^3 field (128 planes: two full work items and a short one along z) and the
+    candidates of mkfTune; every work item is shifted inside the field (X >= 32, Y > 8). The
+    reference's interface rounds thresholds to float (binMapUtil.c:37), so both sides are given
+    the float-rounded thresholds."""
+    import torch
+
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    if repo not in sys.path:
+        sys.path.insert(0, repo)
+    import bench
+
+    Z = 300
+    f = bench.grf_torch(Z, 1024, 1024, 21, cuda)
+    t = np.linspace(-2, 2, 16).astype(np.float32).astype(np.float64)
+    host = np.ascontiguousarray(f.cpu().numpy().ravel())  # X = 1024: the reference reads no slack
+    threads = max(1, len(os.sched_getaffinity(0)))
+    want = np.stack([ref_oracle.bpfd_mt(host, (1024, 1024, Z), float(tv), mkf.BMC_GT, threads) for tv in t])
+    assert (want.sum(axis=1) == 1023 * 1023 * (Z - 1)).all()
+    del host
+    for depth in (None, 128, 64, 32, 8, 4):
+        if depth is not None:
+            mkf.tune(f, t, mkf.BMC_GT, depth=depth)
+        got = u64(mkf.field_bpfd(f, t, mkf.BMC_GT))
+        assert (got == want).all(), depth
+    mkf.tune(f, t, mkf.BMC_GT)
+    assert (u64(mkf.field_bpfd(f, t, mkf.BMC_GT)) == want).all()
+    mkf.tune(f, t, mkf.BMC_GT, depth=0)
+    del f
+    torch.cuda.empty_cache()

@@ -52,6 +52,37 @@ def test_no_alloc_matches_allocating_entry_point(mkf, cuda):
         assert (got == want).all()
 
 
+_CASES = {
+    # FP32, 8 thresholds of '<=' (rank table, rank counts thresholds below or at the value)
+    "f32_le_k8": ((40, 60, 90), np.float32, list(np.linspace(-1.5, 1.5, 8)), 3),
+    # one and two thresholds of '>=' (the word-parallel kernel, as in mkfFieldBPFD)
+    "f32_ge_k1": ((50, 64, 100), np.float32, [0.1], 6),
+    "f64_ge_k2": ((30, 40, 70), np.float64, [-0.4, 0.3], 6),
+    # FP64, 16 thresholds of '<' (rank table, complemented codes)
+    "f64_lt_k16": ((25, 33, 47), np.float64, list(np.linspace(-2, 2, 16)), 1),
+    # a field smaller than one work item, and one of a single plane (no cells)
+    "f64_small": ((3, 7, 5), np.float64, [-0.5, 0.0, 0.5], 4),
+    "f32_one_plane": ((1, 30, 40), np.float32, [0.0, 0.2, 0.4], 4),
+    # every threshold a constant map: nothing is copied
+    "f32_constant": ((6, 9, 11), np.float32, [0.0, float("nan"), 1.0], [7, 2, 0]),
+}
+
+
+@pytest.mark.parametrize("case", sorted(_CASES))
+def test_no_alloc_matches_allocating_entry_point_per_kernel(mkf, cuda, case):
+    """Each kernel route of the no-allocation path (word kernel, rank table for every relation,
+    tiny fields, constant maps) equals mkfFieldBPFDHost exactly, twice in a row."""
+    shape, dtype, t, m = _CASES[case]
+    rng = np.random.default_rng(sum(case.encode()))
+    f = rng.standard_normal(shape).astype(dtype)
+    rc, want = _call(mkf, "host", f, t, m)
+    assert rc == 0, mkf.lib().mkfLastError()
+    for _ in range(2):
+        rc, got = _call(mkf, "noalloc", f, t, m)
+        assert rc == 0, mkf.lib().mkfLastError()
+        assert (got == want).all(), case
+
+
 def test_no_alloc_rejects_planes_beyond_the_staging_area(mkf, cuda):
     # 2048 x 2048 FP64 planes are 32 MiB: two of them do not fit the 32 MiB staging area. The
     # check happens before any device work, so a descriptor of the right size is enough.
