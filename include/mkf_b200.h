@@ -194,6 +194,13 @@ int mkfSetTuning(int batchPlans);
  * entry. Counts the field once to learn which kernels it takes (synchronous). */
 int mkfTuneSet(const MKFFieldDesc *pF, const MKFThreshSet *pT, int depth, void *stream);
 
+/* ---- kernel waits (no original counterpart) ----
+ * The kernels that wait on their own asynchronous copies give every wait a limit; a wait that
+ * runs out (never in a correct run) ends the kernel early, leaves its counts incomplete and sets a
+ * device flag instead of hanging the GPU. mkfKernelFaults returns that flag (0 = none; negative =
+ * an MKF_ERR_* code) and clears it when `clear` is nonzero. Synchronous. */
+int mkfKernelFaults(int clear);
+
 /* ---- measures (closest original: mkfSelectMeasuresBPFD, mkfUtil.c:94) ---- */
 /* For each of nSets distributions (host uint64_t[nSets][256]) write, in double:
  *   r[4*i+0] V   = number of cells whose corner 0 is set (volume in cell units)

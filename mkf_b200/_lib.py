@@ -131,6 +131,7 @@ _SIG = [
     ("mkfBatchBPFD", C.c_int, [_P, C.POINTER(MKFFieldDesc), C.POINTER(MKFThreshSet), C.c_int, C.c_int, _P]),
     ("mkfTune", C.c_int, [C.POINTER(MKFFieldDesc), C.POINTER(MKFThreshSet), _P]),
     ("mkfSetTuning", C.c_int, [C.c_int]),
+    ("mkfKernelFaults", C.c_int, [C.c_int]),
     ("mkfTuneSet", C.c_int, [C.POINTER(MKFFieldDesc), C.POINTER(MKFThreshSet), C.c_int, _P]),
     ("mkfServerCreate", C.c_int, [C.POINTER(C.c_void_p), C.POINTER(MKFServerConfig)]),
     ("mkfServerSubmit", C.c_int, [_P, C.POINTER(MKFRequest), C.POINTER(C.c_uint64)]),

@@ -108,7 +108,7 @@ int planBatchField(const MKFFieldDesc *pF, const MKFThreshSet *pT, int rowBase, 
 
 // Slab depth (planes of cells per work item) of a single-field launch of kernel family `family`
 // (tune.cu): the depth mkfTune measured best for this kind of field, else `def`.
-enum { kFamWords = 0, kFamThermo = 1 };
+enum { kFamWords = 0, kFamThermo = 1, kFamThermoTma = 2 };
 int tunedDepth(int family, int enc, int K, int X, int Y, int Z, int def);
 // The untuned slab depth: def halved (down to 4) until a field of itemsPerPlane work items per
 // plane and Z planes has at least minItems items.

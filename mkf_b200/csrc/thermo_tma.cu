@@ -1,0 +1,520 @@
+// thermo_tma.cu - the rank-table counting kernel with plane tiles staged by TMA, for 3..16
+// thresholds of one relation (< <= > >=) on fields whose rows start on 16-byte boundaries.
+//
+// The method is thermo.cu's (sorted thresholds: an element's K map bits are a thermometer, found
+// as a rank through a table over order-preserving keys; a cell is all-ones below its smallest
+// corner rank, all-zeros from its largest, and mixed codes exist only in between), with the data
+// movement and the per-cell arithmetic rebuilt for the B200:
+//  * Each warp owns a ring of plane tiles in shared memory (34 or 36 x positions, 9 rows) filled
+//    by cp.async.bulk.tensor (TMA) ahead of the plane it counts; an element is one shared-memory
+//    load at a fixed offset, with no per-row address arithmetic, and the next plane's copy is in
+//    flight while the current one is counted. The tensor map covers this GPU's own field only; no
+//    load uses cluster multicast. Every wait on a copy has a poll limit (mkfKernelFaults).
+//  * With K <= 16 an element's thermometer T (bits k < rank) and its complement fit one word,
+//    V = T | ~T << 16. AND over a cell's eight corners gives C = T(min) | ~T(max) << 16 in three
+//    logic operations per cell (x pair, face, cell); popc(C) = 16 - (max - min) is the number of
+//    thresholds the cell does not cross and popc of the low half is its smallest rank.
+//  * All-ones counts: each cell adds 1 to the spare 257th word of its smallest rank's histogram
+//    row (one atomic at a fixed offset from the row address the codes use); the cells all-ones for
+//    threshold k are those whose smallest rank exceeds k, a suffix sum at the flush.
+//  * Mixed codes for k = min, min + 1, min + 2 come from two bit-planes of the corner ranks
+//    relative to min; each goes to the shared [K][257] histogram with an unpredicated atomic whose
+//    address is the code's top byte masked in place plus the row. Where the cell crosses q or
+//    fewer thresholds the code of slot q is 0, and those counts land in bins the flush skips (and
+//    in discard rows past K). Cells crossing four or more thresholds (about 1 in 100 on a smooth
+//    field) are queued per warp with a ballot; the queue is drained 32 cells at a time, taking
+//    back their three slot counts and counting every code they have.
+// Masked cells (lanes and rows outside the item) enter C as all ones: they cross nothing, land in
+// smallest-rank row 16, and are subtracted from the all-ones counts at the flush.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include "thermo.cuh"
+
+namespace mkf {
+
+#ifndef TMA_WARPS
+#define TMA_WARPS 20
+#endif
+#ifndef TMA_STAGES_F64
+#define TMA_STAGES_F64 2
+#endif
+#ifndef TMA_STAGES_F32
+#define TMA_STAGES_F32 3
+#endif
+static constexpr int kTmWarps = TMA_WARPS;
+static constexpr int kTmRows = 9;           // rows of a plane tile: 8 row pairs
+// wide-cell queue entries per warp: a plane adds at most 8 x 31, drained once 32 are waiting (plus
+// one discard entry)
+static constexpr int kTmQueue = 32 + 4 * 31;  // drained after every fourth row
+static constexpr int kTmMaxK = 16;          // thresholds a 16-bit thermometer holds
+static constexpr long kTmWaitLimit = 1L << 22;  // mbarrier polls before a wait gives up
+static constexpr int kTmMaxDepth = kThMaxDepth;  // planes per work item
+
+// Element type geometry: tile width (x positions, a multiple of 16 bytes that covers 32 lanes
+// plus the alignment shift of the tile's first x), stages in the ring, bytes per stage.
+template <typename T>
+struct TmaGeom
+{
+   static constexpr int BX = sizeof(T) == 8 ? 34 : 36;
+   static constexpr int ALIGN = 16 / (int)sizeof(T);  // x coordinates of a TMA tile: multiples of this
+   static constexpr int STAGES = sizeof(T) == 8 ? TMA_STAGES_F64 : TMA_STAGES_F32;
+   static constexpr int BYTES = BX * kTmRows * (int)sizeof(T);   // bytes one TMA copy writes
+   static constexpr int PITCH = (BYTES + 127) / 128 * 128;       // stage stride
+};
+
+// Set when a wait of this kernel ran out of polls (never in a correct run); read by mkfKernelFaults.
+__device__ unsigned gTmaFault;
+
+__device__ __forceinline__ void mbarInit(uint32_t bar, uint32_t count)
+{
+   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+// Lane 0: announce the bytes of the next phase and start the copy of one plane tile.
+__device__ __forceinline__ void tmaPlane(const CUtensorMap *tm, uint32_t dst, uint32_t bar, int x, int y, int z,
+                                         uint32_t bytes)
+{
+   // the stage was last read through the generic proxy; order those reads before the async write
+   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+   asm volatile(
+       "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
+       "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(z), "r"(bar)
+       : "memory");
+}
+
+// Wait for phase `parity` of a barrier; false after kTmWaitLimit polls.
+__device__ __forceinline__ bool mbarWait(uint32_t bar, uint32_t parity)
+{
+   for (long i = 0; i < kTmWaitLimit; i++) {
+      uint32_t done;
+      asm volatile(
+          "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+          : "=r"(done)
+          : "r"(bar), "r"(parity)
+          : "memory");
+      if (done) { return true; }
+   }
+   return false;
+}
+
+
+// Histogram rows per copy: K real rows, then discard rows up to max(K, 16) + 2, where the slots
+// of cells that cross fewer than three thresholds (and of masked cells, whose low half is 16 set
+// bits) add their code-0 counts; the flush reads rows < K and codes 1..254 only.
+__host__ __device__ constexpr int tmaCopyRows(int K) { return (K > 16 ? K : 16) + 3; }
+
+// Exact rank of the element at p by binary search over the sorted thresholds (rare: ties of FP64
+// high words, infinities, NaNs, huge magnitudes). Out of line: it runs only when the fast path
+// flags an element, and one copy serves every row.
+template <typename T, bool GE>
+__device__ __noinline__ uint32_t exactRankAt(const T *p, const double *sTlo, const double *sThi, int K, uint32_t nanRank)
+{
+   const T v = *p;
+   uint32_t r = 0;
+#pragma unroll
+   for (int s = 16; s >= 1; s >>= 1) {
+      if (v > sTlo[r + s - 1]) { r += s; }
+   }
+   if (r > (uint32_t)K) { r = K; }
+   if (GE) {
+      while (r < (uint32_t)K && v >= sThi[r]) { ++r; }
+   }
+   return (v != v) ? nanRank : r;
+}
+
+// Word offset of a code held in the top byte of c (bits below masked off), added to base: one
+// multiply-high with an addend.
+__device__ __forceinline__ uint32_t codeAddr(uint32_t c, uint32_t base) { return __umulhi(c, 1024u) + base; }
+
+// Count the queued wide cells (spread >= 4) of a warp: lane i takes entries i, i + 32, ...; an
+// entry is the cell's two faces of corner ranks (bytes), its smallest rank and spread follow from
+// them. The row loop added three codes for each of them from two rank bit-planes, which are wrong
+// past a spread of 3; they are taken back here (the same formulas, minus one), then every code
+// k = rmin .. rmax - 1 is counted: fixed formulas up to a spread of 7, one threshold at a time
+// beyond (thermo.cu counts them the same way).
+__device__ __noinline__ void drainWide(const uint2 *q, int n, uint32_t hist32)
+{
+   __syncwarp();
+   const int lane = threadIdx.x & 31;
+   for (int i = lane; i < n; i += 32) {
+      const uint2 e = q[i];
+      const uint32_t R0 = e.x, R1 = e.y;
+      uint32_t rmin = 255, rmax = 0;
+#pragma unroll
+      for (int b = 0; b < 4; b++) {
+         const uint32_t u = (R0 >> (8 * b)) & 255u, v = (R1 >> (8 * b)) & 255u;
+         rmin = min(rmin, min(u, v));
+         rmax = max(rmax, max(u, v));
+      }
+      const uint32_t spread = rmax - rmin;
+      const uint32_t rowAddr = hist32 + rmin * (kHistRow * 4);
+      const uint32_t D0 = R0 + rmin * 0xFEFEFEFFu, D1s = R1 * 16u + rmin * 0xEFEFEFF0u;
+      {
+         const uint32_t U = D0 | D1s;
+         const uint32_t G0 = (U & 0x11111111u) * 0x01020408u, G1 = (U & 0x22222222u) * 0x00810204u;
+         const uint32_t a0 = codeAddr((G0 | G1) & 0xFF000000u, rowAddr);
+         const uint32_t a1 = codeAddr(G1 & 0xFF000000u, rowAddr);
+         const uint32_t a2 = codeAddr((G0 & G1) & 0xFF000000u, rowAddr);
+         asm volatile("red.shared.add.u32 [%0], -1;" ::"r"(a0) : "memory");
+         asm volatile("red.shared.add.u32 [%0+%1], -1;" ::"r"(a1), "n"(kHistRow * 4) : "memory");
+         asm volatile("red.shared.add.u32 [%0+%1], -1;" ::"r"(a2), "n"(kHistRow * 8) : "memory");
+      }
+      if (spread < 8) {
+         const uint32_t b0 = gatherBits((D0 & 0x01010101u) | (D1s & 0x10101010u), 0x01020408u);
+         const uint32_t b1 = gatherBits((D0 & 0x02020202u) | (D1s & 0x20202020u), 0x00810204u);
+         const uint32_t b2 = gatherBits((D0 & 0x04040404u) | (D1s & 0x40404040u), 0x00408102u);
+         redSharedAt<0>((b0 | b1 | b2) * 4u + rowAddr);
+         redSharedAt<kHistRow * 4>((b1 | b2) * 4u + rowAddr);
+         redSharedAt<kHistRow * 8>((b2 | (b1 & b0)) * 4u + rowAddr);
+         redSharedAt<kHistRow * 12>(b2 * 4u + rowAddr);
+         if (spread > 4) { redSharedAt<kHistRow * 16>((b2 & (b1 | b0)) * 4u + rowAddr); }
+         if (spread > 5) { redSharedAt<kHistRow * 20>((b2 & b1) * 4u + rowAddr); }
+         if (spread > 6) { redSharedAt<kHistRow * 24>((b2 & b1 & b0) * 4u + rowAddr); }
+      } else {
+         uint32_t C = 0x7F7F7F7Fu - rmin * 0x01010101u, addr = rowAddr;
+         for (uint32_t k = 0; k < spread; ++k) {
+            redShared(addr + (cellCode(R0, R1, C) << 2));
+            C -= 0x01010101u;
+            addr += kHistRow * 4;
+         }
+      }
+   }
+   __syncwarp();
+}
+
+// Geometry of one work item: 31 x positions of cells, 8 row pairs, up to D planes of cells.
+struct TmItem
+{
+   int xa, xoff;     // tile x (a multiple of ALIGN) and this item's first lane column in it
+   int y0, z0, nPln; // tile rows y0 .. y0 + 8, planes z0 .. z0 + nPln
+   uint32_t rowsOK;  // bit j: this lane counts row pair j
+   unsigned cells;   // cells the item counts (warp total)
+};
+
+template <int ALIGN>
+__device__ __forceinline__ TmItem itemOf(const FusedArgs &a, long long it, int lane)
+{
+   TmItem m;
+   const int ix = (int)(it % a.nSegX);
+   const long long rest = it / a.nSegX;
+   const int iy = (int)(rest % a.nTileY);
+   const int iz = (int)(rest / a.nTileY);
+   const int xs = 31 * ix, ys = 8 * iy;
+   const int xe = min(xs + 31, a.X - 1), ye = min(ys + 8, a.Y - 1);
+   const int x0 = min(xs, a.X - 32);  // lanes at x0 + lane, all inside the field
+   m.xa = x0 & ~(ALIGN - 1);
+   m.xoff = x0 - m.xa;
+   m.y0 = min(ys, a.Y - 9);
+   m.z0 = a.D * iz;
+   m.nPln = min(a.D, a.Z - 1 - m.z0);
+   const int jlo = ys - m.y0, jhi = ye - m.y0;
+   const bool laneIn = x0 + lane >= xs && x0 + lane < xe;
+   m.rowsOK = laneIn ? (((1u << jhi) - 1u) & ~((1u << jlo) - 1u)) : 0u;
+   m.cells = (unsigned)(xe - xs) * (unsigned)(jhi - jlo) * (unsigned)m.nPln;
+   return m;
+}
+
+template <typename T, bool GE, int CMAX>
+__global__ void __launch_bounds__(kTmWarps * 32, 1)
+    thermoTmaBPFD(const __grid_constant__ FusedArgs a, const __grid_constant__ CUtensorMap tm)
+{
+   using G = TmaGeom<T>;
+   constexpr int W = sizeof(T) / 4;   // 32-bit words per element; the ranked word is the last
+   constexpr int S = G::STAGES;
+   __shared__ ThermoShared Sh;
+   __shared__ alignas(8) uint64_t bars[kTmWarps][G::STAGES];
+   extern __shared__ __align__(128) unsigned char dsm[];
+   const int K = a.K;
+   const int copyRows = tmaCopyRows(K);
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   uint32_t *hist = reinterpret_cast<uint32_t *>(dsm);
+   const size_t histBytes = ((size_t)copyRows * kHistRow * kHistCopies * 4 + 127) / 128 * 128;
+   // the ring starts on a 128-byte boundary (TMA destination), whatever the dynamic base's alignment
+   // (offset from dsm, so that the compiler keeps these pointers in the shared window)
+   const uint32_t histEnd = (uint32_t)__cvta_generic_to_shared(dsm) + (uint32_t)histBytes;
+   unsigned char *ring = dsm + histBytes + ((128u - (histEnd & 127u)) & 127u);
+   uint2 *queue = reinterpret_cast<uint2 *>(ring + (size_t)kTmWarps * S * G::PITCH) + warp * (kTmQueue + 1);
+
+   if (lane == 0) {
+      for (int s = 0; s < S; s++) { mbarInit((uint32_t)__cvta_generic_to_shared(&bars[warp][s]), 1); }
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+   }
+   ctaSetup(a, Sh, hist, copyRows);  // (its barriers also order the mbarrier set-up)
+
+   const uint32_t ringW = (uint32_t)__cvta_generic_to_shared(ring) + (uint32_t)(warp * S * G::PITCH);
+   const uint32_t bar0 = (uint32_t)__cvta_generic_to_shared(&bars[warp][0]);
+   const uint32_t histBase = (uint32_t)__cvta_generic_to_shared(hist);
+   const uint32_t hist32 = histBase + (uint32_t)((lane & (kHistCopies - 1)) * copyRows * kHistRow) * 4u;
+   const uint32_t nanRank = a.nanRank;
+   const uint32_t lanesBelow = (1u << lane) - 1u;
+   const long long nw = (long long)gridDim.x * kTmWarps;
+   const long long first = (long long)blockIdx.x * kTmWarps + warp;
+
+   // producer cursor (every lane tracks it; lane 0 issues): item, plane, tile coordinates
+   long long pIt = first;
+   int pP = 0, pX = 0, pY = 0, pZ = 0, pN = -1;
+   if (pIt < a.nItems) {
+      const TmItem m = itemOf<G::ALIGN>(a, pIt, lane);
+      pX = m.xa; pY = m.y0; pZ = m.z0; pN = m.nPln;
+   }
+   uint32_t gp = 0;  // planes issued by this warp
+   auto issue = [&]() {
+      if (pIt >= a.nItems) { return; }
+      if (lane == 0) {
+         const uint32_t st = gp % S;
+         tmaPlane(&tm, ringW + st * G::PITCH, bar0 + 8u * st, pX, pY, pZ + pP, G::BYTES);
+      }
+      ++gp;
+      if (++pP > pN) {
+         pIt += nw;
+         pP = 0;
+         if (pIt < a.nItems) {
+            const TmItem m = itemOf<G::ALIGN>(a, pIt, lane);
+            pX = m.xa; pY = m.y0; pZ = m.z0; pN = m.nPln;
+         }
+      }
+   };
+   for (int s = 0; s + 1 < S; s++) { issue(); }
+
+   uint32_t g = 0;  // planes consumed by this warp
+   bool fault = false;
+   // wait for plane g's tile, rank the lane's column (9 rows), refill the stage of plane g - 1
+   auto plane = [&](int xoff, uint32_t (&r)[kTmRows]) -> bool {
+      const uint32_t st = g % S;
+      if (!mbarWait(bar0 + 8u * st, (g / S) & 1u)) { return false; }
+      // this lane's column of the plane tile (the mbarrier wait orders these loads after the copy)
+      const T *col = reinterpret_cast<const T *>(ring + (size_t)(warp * S + (int)st) * G::PITCH) + xoff + lane;
+      const uint32_t *colW = reinterpret_cast<const uint32_t *>(col) + (W - 1);
+      bool slow = false;
+#pragma unroll
+      for (int j = 0; j < kTmRows; ++j) {
+         const uint32_t key = sortKey(colW[j * G::BX * W]);
+         const uint32_t r0 = Sh.lut[key >> kLutShift];
+         const uint32_t cand = Sh.key[r0];
+         uint32_t rr = r0 + (GE ? (key >= cand) : (key > cand));
+         bool tie = key == cand;
+#pragma unroll
+         for (int c = 1; c < CMAX; ++c) {
+            const uint32_t cc = Sh.key[r0 + c];
+            rr += GE ? (key >= cc) : (key > cc);
+            tie = tie | (key == cc);
+         }
+         slow = slow | (W == 2 && tie) | (r0 >= kSlowBucket);
+         r[j] = rr;
+      }
+      if (__any_sync(FULL, slow)) {
+         if (slow) {
+#pragma unroll
+            for (int j = 0; j < kTmRows; ++j) { r[j] = exactRankAt<T, GE>(col + j * G::BX, Sh.tlo, Sh.thi, K, nanRank); }
+         }
+      }
+      __syncwarp();
+      issue();  // refill the stage of the previous plane (read by every lane by now)
+      ++g;
+      return true;
+   };
+   // thermometer of a rank and its complement: T | ~T << 16, T = bits [0, r)
+   auto thermoV = [](uint32_t r) { return thermo(r) * 0xFFFF0001u + 0xFFFF0000u; };
+
+   unsigned long long cells = 0;
+   uint32_t masked = 0;  // masked cells counted (in smallest-rank row 16)
+   int qn = 0;           // wide cells queued
+   for (long long it = first; it < a.nItems; it += nw) {
+      const TmItem m = itemOf<G::ALIGN>(a, it, lane);
+      cells += m.cells;
+      masked += (8u - (uint32_t)__popc(m.rowsOK)) * (uint32_t)m.nPln;
+      uint32_t sF[8], sV[8];  // previous plane: face ranks (bytes), face thermometer AND
+      {
+         uint32_t r[kTmRows];
+         if (!plane(m.xoff, r)) { fault = true; break; }
+         uint32_t rR = __shfl_down_sync(FULL, r[0], 1);
+         uint32_t V = thermoV(r[0]), VR = __shfl_down_sync(FULL, V, 1);
+         uint32_t ePrev = rR * 256u + r[0], Pprev = V & VR;
+#pragma unroll
+         for (int j = 0; j < 8; ++j) {
+            rR = __shfl_down_sync(FULL, r[j + 1], 1);
+            V = thermoV(r[j + 1]);
+            VR = __shfl_down_sync(FULL, V, 1);
+            const uint32_t e = rR * 256u + r[j + 1], P = V & VR;
+            sF[j] = e * 65536u + ePrev;
+            sV[j] = P & Pprev;
+            ePrev = e;
+            Pprev = P;
+         }
+      }
+      for (int p = 1; p <= m.nPln; ++p) {
+         uint32_t r[kTmRows];
+         if (!plane(m.xoff, r)) { fault = true; break; }
+         uint32_t rR = __shfl_down_sync(FULL, r[0], 1);
+         uint32_t V = thermoV(r[0]), VR = __shfl_down_sync(FULL, V, 1);
+         uint32_t ePrev = rR * 256u + r[0];
+         uint32_t Pprev = V & VR;
+#pragma unroll
+         for (int j = 0; j < 8; ++j) {
+            rR = __shfl_down_sync(FULL, r[j + 1], 1);
+            V = thermoV(r[j + 1]);
+            VR = __shfl_down_sync(FULL, V, 1);
+            const uint32_t e = rR * 256u + r[j + 1];
+            const uint32_t P = V & VR;
+            const uint32_t fc = e * 65536u + ePrev;  // face ranks: (x,y) (x+1,y) (x,y+1) (x+1,y+1)
+            const uint32_t F = P & Pprev;
+            const uint32_t nvm = ((m.rowsOK >> j) & 1u) - 1u;  // all ones for a masked cell
+            const uint32_t C = (F & sV[j]) | nvm;
+            const uint32_t pc = __popc(C), rmin = __popc(C & 0xFFFFu);
+            const uint32_t R0 = sF[j], R1 = fc;
+            const uint32_t D0 = R0 + rmin * 0xFEFEFEFFu;         // R0 - rmin per byte
+            const uint32_t D1s = R1 * 16u + rmin * 0xEFEFEFF0u;  // (R1 - rmin per byte) << 4
+            // bits 0 and 1 of each corner's rank - rmin (below 4 unless the cell is wide): byte b
+            // of U holds face z's corner in bits 0-1 and face z + 1's in bits 4-5
+            const uint32_t U = D0 | D1s;
+            const uint32_t G0 = (U & 0x11111111u) * 0x01020408u;
+            const uint32_t G1 = (U & 0x22222222u) * 0x00810204u;
+            const uint32_t rowAddr = hist32 + rmin * (kHistRow * 4);
+            // codes k = rmin + q mark the corners with rank - rmin > q: b0 | b1, b1, b0 & b1 (the
+            // top bytes of G0, G1); a code is 0 where the cell crosses q or fewer thresholds, and
+            // such counts land in discard bins
+            redSharedAt<0>(codeAddr((G0 | G1) & 0xFF000000u, rowAddr));
+            redSharedAt<kHistRow * 4>(codeAddr(G1 & 0xFF000000u, rowAddr));
+            redSharedAt<kHistRow * 8>(codeAddr((G0 & G1) & 0xFF000000u, rowAddr));
+            redSharedAt<256 * 4>(rowAddr);  // the cell's smallest rank (word 256 of the row)
+            const bool wide = pc < 13u;  // crosses 4 or more thresholds
+            const uint32_t wb = __ballot_sync(FULL, wide);  // warp-uniform: the branch below is too
+            if (wb) {
+               // every lane stores; the others into the discard entry
+               queue[wide ? qn + __popc(wb & lanesBelow) : kTmQueue] = make_uint2(R0, R1);
+               qn += __popc(wb);
+            }
+            sF[j] = fc;
+            sV[j] = F;
+            ePrev = e;
+            Pprev = P;
+            if ((j & 3) == 3 && qn >= 32) {
+               drainWide(queue, qn, hist32);
+               qn = 0;
+            }
+         }
+      }
+      if (fault) { break; }
+      if (qn > 0) {
+         drainWide(queue, qn, hist32);
+         qn = 0;
+      }
+   }
+   if (fault) {
+      if (lane == 0) { atomicOr(&gTmaFault, 1u); }
+      // let the copies this warp started finish before its shared memory is released
+      for (uint32_t q = g; q < gp; ++q) { mbarWait(bar0 + 8u * (q % S), (q / S) & 1u); }
+   }
+   if (lane == 0 && cells) { atomicAdd(&Sh.cells, cells); }
+   masked = __reduce_add_sync(FULL, masked);  // (per lane: its own masked row pairs)
+   if (lane == 0 && masked) { atomicAdd(&Sh.ones[MKF_MAX_THRESH - 1], masked); }
+   __syncthreads();
+   // all-ones counts: cells whose smallest rank exceeds k, less the masked cells (rank 16)
+   if (threadIdx.x < (unsigned)K) {
+      const int k = threadIdx.x;
+      uint32_t n = 0;
+      for (int r = k + 1; r <= kTmMaxK; r++) {
+#pragma unroll
+         for (int q = 0; q < kHistCopies; ++q) { n += hist[(q * copyRows + r) * kHistRow + 256]; }
+      }
+      Sh.ones[k] = n - Sh.ones[MKF_MAX_THRESH - 1];
+   }
+   ctaFlush(a, Sh, hist, copyRows);
+}
+
+// ---------------------------------------------------------------- host
+
+template <typename T>
+static size_t tmaDynBytes(int K)
+{
+   using G = TmaGeom<T>;
+   const size_t histBytes = ((size_t)tmaCopyRows(K) * kHistRow * kHistCopies * 4 + 127) / 128 * 128;
+   return histBytes + 128 + (size_t)kTmWarps * G::STAGES * G::PITCH + (size_t)kTmWarps * (kTmQueue + 1) * sizeof(uint2);
+}
+
+static PFN_cuTensorMapEncodeTiled_v12000 encodeFn()
+{
+   static std::once_flag once;
+   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+   std::call_once(once, [] {
+      void *p = nullptr;
+      cudaDriverEntryPointQueryResult q;
+      if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+          q == cudaDriverEntryPointSuccess) {
+         fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+      } else {
+         cudaGetLastError();
+      }
+   });
+   return fn;
+}
+
+template <typename T, bool GE, int CMAX>
+static int launchTmaT(const FusedArgs &a, const CUtensorMap &tm, cudaStream_t s)
+{
+   static std::atomic<int> occ[kTmMaxK + 1];
+   auto kern = thermoTmaBPFD<T, GE, CMAX>;
+   const size_t smem = tmaDynBytes<T>(a.K);
+   const int blocksPerSM = cachedOccupancy(occ[a.K], kern, kTmWarps * 32, smem, tmaDynBytes<T>(kTmMaxK));
+   long long grid = (a.nItems + kTmWarps - 1) / kTmWarps;
+   const long long cap = (long long)smCount() * blocksPerSM;
+   if (grid > cap) { grid = cap; }
+   if (grid < 1) { grid = 1; }
+   kern<<<(unsigned)grid, kTmWarps * 32, smem, s>>>(a, tm);
+   return cudaFail(cudaGetLastError(), "thermoTmaBPFD launch");
+}
+
+template <typename T, bool GE>
+static int launchTmaG(const FusedArgs &a, const CUtensorMap &tm, cudaStream_t s)
+{
+   return a.lutC > 1 ? launchTmaT<T, GE, 4>(a, tm, s) : launchTmaT<T, GE, 1>(a, tm, s);
+}
+
+bool thermoTmaEligible(const FusedArgs &a, int enc)
+{
+   const int64_t esz = enc == ENC_F32 ? 4 : 8;
+   return a.K > 2 && a.K <= kTmMaxK && a.lutC >= 1 && a.sx == 1 && a.X >= 32 && a.Y >= 9 && a.Z >= 2 &&
+          ((uintptr_t)a.f % 16) == 0 && (a.sy * esz) % 16 == 0 && (a.sz * esz) % 16 == 0 && a.sy >= a.X &&
+          a.sz >= a.sy * a.Y && a.D >= 1 && a.D <= kTmMaxDepth && encodeFn() != nullptr;
+}
+
+// a.tkey / a.lutC filled (prepareKeys) and the item grid set for 8-row items (itemGrid).
+int launchThermoTma(const FusedArgs &a, int enc, cudaStream_t s)
+{
+   if (!thermoTmaEligible(a, enc)) { return MKF_ERR_UNSUPPORTED; }
+   const bool f32 = enc == ENC_F32;
+   const cuuint64_t esz = f32 ? 4 : 8;
+   CUtensorMap tm;
+   const cuuint64_t dims[3] = {(cuuint64_t)a.X, (cuuint64_t)a.Y, (cuuint64_t)a.Z};
+   const cuuint64_t strides[2] = {(cuuint64_t)a.sy * esz, (cuuint64_t)a.sz * esz};
+   const cuuint32_t box[3] = {(cuuint32_t)(f32 ? TmaGeom<float>::BX : TmaGeom<double>::BX), (cuuint32_t)kTmRows, 1};
+   const cuuint32_t estr[3] = {1, 1, 1};
+   const CUresult cr = encodeFn()(&tm, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+                                  const_cast<void *>(a.f), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+   if (cr != CUDA_SUCCESS) { return MKF_ERR_UNSUPPORTED; }
+   const bool ge = a.rankHi != 0;
+   if (f32) { return ge ? launchTmaG<float, true>(a, tm, s) : launchTmaG<float, false>(a, tm, s); }
+   return ge ? launchTmaG<double, true>(a, tm, s) : launchTmaG<double, false>(a, tm, s);
+}
+
+}  // namespace mkf
+
+MKF_API int mkfKernelFaults(int clear)
+{
+   unsigned v = 0;
+   cudaError_t e = cudaMemcpyFromSymbol(&v, mkf::gTmaFault, sizeof(v));
+   if (e != cudaSuccess) { return mkf::cudaFail(e, "mkfKernelFaults"); }
+   if (clear && v) {
+      const unsigned z = 0;
+      e = cudaMemcpyToSymbol(mkf::gTmaFault, &z, sizeof(z));
+      if (e != cudaSuccess) { return mkf::cudaFail(e, "mkfKernelFaults"); }
+   }
+   return (int)v;
+}

@@ -774,3 +774,78 @@ def test_benchmark_config_equals_reference_c_path(mkf, ref_oracle, cuda):
     mkf.tune(f, t, mkf.BMC_GT, depth=0)
     del f
     torch.cuda.empty_cache()
+
+
+# ---------------------------------------------------------------- the TMA-staged rank-table kernel
+
+def _smooth(rng, shape, dtype):
+    f = rng.standard_normal(shape)
+    for ax in range(3):
+        f = f + np.roll(f, 1, axis=ax)
+    return (f / f.std()).astype(dtype)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_tma_rank_table_kernel_against_oracle(mkf, oracle, cuda, dtype):
+    """Fields whose rows start on 16-byte boundaries (X a multiple of 4 for FP32, of 2 for FP64)
+    take the TMA-staged rank-table kernel for 7..16 thresholds of one relation. Every relation,
+    edge items in x and y (X - 1 and Y - 1 not multiples of 31 and 8), a field of exactly one item
+    row (Y = 9), a slab ending mid-item, dense thresholds (cells crossing 4 to 16 of them: the
+    queued wide cells), thresholds sharing rank-table buckets (four candidates), and a view with
+    aligned strides, against the oracle; no kernel wait ran out."""
+    import torch
+
+    rng = np.random.default_rng(808 if dtype == np.float64 else 809)
+    a = 4 if dtype == np.float32 else 2
+    shapes = [(20, 9, 32), (33, 17, 64), (12, 50, 25 * a), (9, 70, 9 * a), (130, 12, 10 * a)]
+    sets = [np.linspace(-1.5, 1.5, 7), np.linspace(-2, 2, 16), np.linspace(-0.4, 0.4, 16),
+            np.array([0.5, 0.5 + 1e-7, 0.5 + 2e-7, 0.5 + 3e-7, -1.0, 0.0, 1.0, 1.5])]
+    masks = [mkf.BMC_GT, mkf.BMC_GT | mkf.BMC_EQ, mkf.BMC_LT, mkf.BMC_LT | mkf.BMC_EQ]
+    mkf.lib().mkfKernelFaults(1)
+    for i, shape in enumerate(shapes):
+        f = _smooth(rng, shape, dtype)
+        Z, Y, X = shape
+        fd = to_dev(f, cuda)
+        for j, t in enumerate(sets):
+            m = masks[(i + j) % 4]
+            got = u64(mkf.field_bpfd(fd, t, m))
+            assert (got == oracle.bpfd_field(f, (X, Y, Z), t, m)).all(), (shape, j, m)
+    # a view whose strides are multiples of 16 bytes: a sub-box of a larger field
+    big = _smooth(rng, (40, 30, 16 * a), dtype)
+    bd = to_dev(big, cuda)
+    view = bd[3:35, 2:27, :12 * a]
+    sub = np.ascontiguousarray(big[3:35, 2:27, :12 * a])
+    t = np.linspace(-1.2, 1.2, 11)
+    got = u64(mkf.field_bpfd(view, t, mkf.BMC_GT))
+    assert (got == oracle.bpfd_field(sub, (12 * a, 25, 32), t, mkf.BMC_GT)).all()
+    assert mkf.lib().mkfKernelFaults(1) == 0
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_tma_rank_table_kernel_exact_path_and_depths(mkf, oracle, cuda, dtype):
+    """The TMA-staged kernel's exact path: elements equal to thresholds (ties of the whole value,
+    and for FP64 of the high word only), infinities, NaNs and huge magnitudes, under every relation;
+    and slab depths from 4 to 255 planes (mkfTuneSet), against the oracle."""
+    rng = np.random.default_rng(77)
+    shape = (70, 20, 64)
+    f = (rng.integers(-8, 9, size=shape) * 0.25).astype(np.float64)
+    flat = f.reshape(-1)
+    idx = rng.permutation(flat.size)
+    flat[idx[:300]] = np.nan
+    flat[idx[300:600]] = np.inf
+    flat[idx[600:900]] = -np.inf
+    flat[idx[900:1000]] = 1e300 if dtype == np.float64 else 3e38
+    flat[idx[1000:1400]] = 0.5 + 1e-12  # same FP64 high word as 0.5
+    f = f.astype(dtype)
+    Z, Y, X = shape
+    fd = to_dev(f, cuda)
+    t = np.arange(-1.75, 2.0, 0.25)  # 15 thresholds on the values' grid: many exact ties
+    for m in (mkf.BMC_GT, mkf.BMC_GT | mkf.BMC_EQ, mkf.BMC_LT, mkf.BMC_LT | mkf.BMC_EQ):
+        want = oracle.bpfd_field(f, (X, Y, Z), t, m)
+        assert (u64(mkf.field_bpfd(fd, t, m)) == want).all(), m
+    want = oracle.bpfd_field(f, (X, Y, Z), t, mkf.BMC_GT)
+    for depth in (4, 8, 64, 128, 255):
+        mkf.tune(fd, t, mkf.BMC_GT, depth=depth)
+        assert (u64(mkf.field_bpfd(fd, t, mkf.BMC_GT)) == want).all(), depth
+    mkf.tune(fd, t, mkf.BMC_GT, depth=0)
+    assert mkf.lib().mkfKernelFaults(1) == 0
