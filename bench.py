@@ -588,7 +588,7 @@ def measured_hbm_peak():
 
 def profiled_traffic():
     """DRAM bytes per launch of the fused kernel from the committed ncu summary, if present."""
-    path = os.path.join(REPO, "profiles", "fused_grf1024_f64_k16.md")
+    path = os.path.join(REPO, "profiles", "thermo_tma_grf_f64_k16.md")
     try:
         for line in open(path):
             if line.startswith("dram_bytes_per_launch_full:"):

@@ -307,7 +307,8 @@ int launchFusedPlain(const FusedPlain &q, cudaStream_t s)
    a.out = q.out;
    // the kernel choice of fieldBPFD: the word-parallel kernel for one or two thresholds, and for a
    // few of one relation
-   const int wordMaxK = std::min(kWordMaxK, q.enc == ENC_F32 ? 5 : 6);
+   int wordMaxK = std::min(kWordMaxK, q.enc == ENC_F32 ? 5 : 6);
+   if (q.thermo && q.K == wordMaxK && tmaRowsAligned(a, q.enc)) { wordMaxK--; }
    if (q.K <= 2 || (q.thermo && q.K <= wordMaxK)) { return launchWords(a, q.enc, q.mask, s); }
    constexpr int TY = 16;
    a.D = 64;
@@ -506,8 +507,10 @@ int fieldBPFD(uint64_t *out, const MKFFieldDesc *pF, const MKFThreshSet *pT, int
       }
       a.out = out;
       // a few thresholds of one relation: one ballot per row and threshold costs less than the
-      // rank table up to 5 (FP32) / 6 (FP64) thresholds (B200, 512^3 Gaussian field)
-      const int wordMaxK = std::min(kWordMaxK, pF->enc == ENC_F32 ? 5 : 6);
+      // rank table up to 5 (FP32) / 6 (FP64) thresholds, and less than the TMA-staged rank table
+      // (16-byte aligned rows) up to 4 / 5 (B200, 512^3 Gaussian field)
+      int wordMaxK = std::min(kWordMaxK, pF->enc == ENC_F32 ? 5 : 6);
+      if (ps.thermo && a.K == wordMaxK && tmaRowsAligned(a, pF->enc)) { wordMaxK--; }
       if (a.K <= 2 || (ps.thermo && a.K <= wordMaxK)) {
          uint32_t masks[MKF_MAX_THRESH];
          for (int k = 0; k < a.K; k++) { masks[k] = ps.mask[idx[k]]; }

@@ -146,6 +146,10 @@ int launchWords(const FusedArgs &f, int enc, const uint32_t *masks, cudaStream_t
 // mom is device double[K][2][2], per threshold and map value the sum of f and of f^2.
 int launchWordsMoments(const FusedArgs &f, int enc, const uint32_t *masks, double *mom, cudaStream_t s);
 
+// Whether a pass's field and threshold count suit the TMA-staged rank-table kernel (thermo_tma.cu):
+// 3..16 thresholds, unit x stride, rows and planes on 16-byte boundaries, X >= 32, Y >= 9.
+bool tmaRowsAligned(const FusedArgs &a, int enc);
+
 // Launch the thermometer kernel for a pass whose thresholds all share one relation
 // (< <= > >=); fills the key table of `a` first.
 int launchThermo(FusedArgs &a, int enc, cudaStream_t s);

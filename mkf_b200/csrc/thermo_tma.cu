@@ -14,9 +14,10 @@
 //    V = T | ~T << 16. AND over a cell's eight corners gives C = T(min) | ~T(max) << 16 in three
 //    logic operations per cell (x pair, face, cell); popc(C) = 16 - (max - min) is the number of
 //    thresholds the cell does not cross and popc of the low half is its smallest rank.
-//  * All-ones counts: each cell adds 1 to the spare 257th word of its smallest rank's histogram
-//    row (one atomic at a fixed offset from the row address the codes use); the cells all-ones for
-//    threshold k are those whose smallest rank exceeds k, a suffix sum at the flush.
+//  * All-ones counts cost no per-cell work: the three code slots add one count each to rows rmin,
+//    rmin + 1 and rmin + 2 (real codes or discarded 0s), so the row totals give, by a recurrence at
+//    the flush, the number of cells of each smallest rank; the cells all-ones for threshold k are
+//    those whose smallest rank exceeds k.
 //  * Mixed codes for k = min, min + 1, min + 2 come from two bit-planes of the corner ranks
 //    relative to min; each goes to the shared [K][257] histogram with an unpredicated atomic whose
 //    address is the code's top byte masked in place plus the row. Where the cell crosses q or
@@ -49,7 +50,7 @@ static constexpr int kTmWarps = TMA_WARPS;
 static constexpr int kTmRows = 9;           // rows of a plane tile: 8 row pairs
 // wide-cell queue entries per warp: a plane adds at most 8 x 31, drained once 32 are waiting (plus
 // one discard entry)
-static constexpr int kTmQueue = 32 + 4 * 31;  // drained after every fourth row
+static constexpr int kTmQueue = 32 + 8 * 31;  // drained after a plane once 32 are waiting
 static constexpr int kTmMaxK = 16;          // thresholds a 16-bit thermometer holds
 static constexpr long kTmWaitLimit = 1L << 22;  // mbarrier polls before a wait gives up
 static constexpr int kTmMaxDepth = kThMaxDepth;  // planes per work item
@@ -183,6 +184,11 @@ __device__ __noinline__ void drainWide(const uint2 *q, int n, uint32_t hist32)
             addr += kHistRow * 4;
          }
       }
+      // row totals count every cell once in rows rmin .. rmin + 2: take back the codes counted in
+      // rows rmin + 3 .. rmax - 1 from those rows' spare word
+      for (uint32_t q = 3; q < spread; ++q) {
+         asm volatile("red.shared.add.u32 [%0+%1], -1;" ::"r"(rowAddr + q * (kHistRow * 4)), "n"(256 * 4) : "memory");
+      }
    }
    __syncwarp();
 }
@@ -228,6 +234,7 @@ __global__ void __launch_bounds__(kTmWarps * 32, 1)
    constexpr int S = G::STAGES;
    __shared__ ThermoShared Sh;
    __shared__ alignas(8) uint64_t bars[kTmWarps][G::STAGES];
+   __shared__ uint32_t rowTot[kTmMaxK + 1];
    extern __shared__ __align__(128) unsigned char dsm[];
    const int K = a.K;
    const int copyRows = tmaCopyRows(K);
@@ -290,7 +297,8 @@ __global__ void __launch_bounds__(kTmWarps * 32, 1)
       // this lane's column of the plane tile (the mbarrier wait orders these loads after the copy)
       const T *col = reinterpret_cast<const T *>(ring + (size_t)(warp * S + (int)st) * G::PITCH) + xoff + lane;
       const uint32_t *colW = reinterpret_cast<const uint32_t *>(col) + (W - 1);
-      bool slow = false;
+      bool slow = false;   // a FP64 high word equal to a threshold's
+      uint32_t rOr = 0;    // slow-path buckets rank above 32
 #pragma unroll
       for (int j = 0; j < kTmRows; ++j) {
          const uint32_t key = sortKey(colW[j * G::BX * W]);
@@ -304,9 +312,12 @@ __global__ void __launch_bounds__(kTmWarps * 32, 1)
             rr += GE ? (key >= cc) : (key > cc);
             tie = tie | (key == cc);
          }
-         slow = slow | (W == 2 && tie) | (r0 >= kSlowBucket);
+         if (W == 2) { slow = slow | tie; }
+         rOr |= rr;
          r[j] = rr;
       }
+      static_assert(kSlowBucket >= 32 && kTmMaxK < 32, "slow buckets rank at 32 or more");
+      slow = slow | (rOr >= 32u);
       if (__any_sync(FULL, slow)) {
          if (slow) {
 #pragma unroll
@@ -381,22 +392,20 @@ __global__ void __launch_bounds__(kTmWarps * 32, 1)
             redSharedAt<0>(codeAddr((G0 | G1) & 0xFF000000u, rowAddr));
             redSharedAt<kHistRow * 4>(codeAddr(G1 & 0xFF000000u, rowAddr));
             redSharedAt<kHistRow * 8>(codeAddr((G0 & G1) & 0xFF000000u, rowAddr));
-            redSharedAt<256 * 4>(rowAddr);  // the cell's smallest rank (word 256 of the row)
-            const bool wide = pc < 13u;  // crosses 4 or more thresholds
-            const uint32_t wb = __ballot_sync(FULL, wide);  // warp-uniform: the branch below is too
-            if (wb) {
-               // every lane stores; the others into the discard entry
-               queue[wide ? qn + __popc(wb & lanesBelow) : kTmQueue] = make_uint2(R0, R1);
-               qn += __popc(wb);
-            }
+            // cells crossing 4 or more thresholds join the warp's queue; every lane stores (the
+            // others into the discard entry), so the row body has no branch
+            const bool wide = pc < 13u;
+            const uint32_t wb = __ballot_sync(FULL, wide);
+            queue[wide ? qn + __popc(wb & lanesBelow) : kTmQueue] = make_uint2(R0, R1);
+            qn += __popc(wb);
             sF[j] = fc;
             sV[j] = F;
             ePrev = e;
             Pprev = P;
-            if ((j & 3) == 3 && qn >= 32) {
-               drainWide(queue, qn, hist32);
-               qn = 0;
-            }
+         }
+         if (qn >= 32) {
+            drainWide(queue, qn, hist32);
+            qn = 0;
          }
       }
       if (fault) { break; }
@@ -414,15 +423,32 @@ __global__ void __launch_bounds__(kTmWarps * 32, 1)
    masked = __reduce_add_sync(FULL, masked);  // (per lane: its own masked row pairs)
    if (lane == 0 && masked) { atomicAdd(&Sh.ones[MKF_MAX_THRESH - 1], masked); }
    __syncthreads();
-   // all-ones counts: cells whose smallest rank exceeds k, less the masked cells (rank 16)
-   if (threadIdx.x < (unsigned)K) {
-      const int k = threadIdx.x;
-      uint32_t n = 0;
-      for (int r = k + 1; r <= kTmMaxK; r++) {
+   // All-ones counts. Every cell counted once in each of rows rmin, rmin + 1, rmin + 2 (a code, a
+   // discarded 0, or for wide cells the drain's corrections), so row r's total over all 257 words
+   // is N[r] + N[r-1] + N[r-2], N[r] the cells whose smallest rank is r; the cells all-ones for
+   // threshold k are those with rmin > k, less the masked cells (rmin 16).
+   for (int r = warp; r <= kTmMaxK; r += kTmWarps) {
+      uint32_t t = 0;
+      for (int c = lane; c < kHistRow; c += 32) {
 #pragma unroll
-         for (int q = 0; q < kHistCopies; ++q) { n += hist[(q * copyRows + r) * kHistRow + 256]; }
+         for (int q = 0; q < kHistCopies; ++q) { t += hist[(q * copyRows + r) * kHistRow + c]; }
       }
-      Sh.ones[k] = n - Sh.ones[MKF_MAX_THRESH - 1];
+      t = __reduce_add_sync(FULL, t);
+      if (lane == 0) { rowTot[r] = t; }
+   }
+   __syncthreads();
+   if (threadIdx.x == 0) {
+      uint32_t n1 = 0, n2 = 0, nr[kTmMaxK + 1];
+      for (int r = 0; r <= kTmMaxK; r++) {
+         nr[r] = rowTot[r] - n1 - n2;
+         n2 = n1;
+         n1 = nr[r];
+      }
+      uint32_t above = nr[kTmMaxK] - Sh.ones[MKF_MAX_THRESH - 1];  // rmin > k, from k = 15 down
+      for (int k = kTmMaxK - 1; k >= 0; k--) {
+         if (k < K) { Sh.ones[k] = above; }
+         above += nr[k];
+      }
    }
    ctaFlush(a, Sh, hist, copyRows);
 }
@@ -475,12 +501,16 @@ static int launchTmaG(const FusedArgs &a, const CUtensorMap &tm, cudaStream_t s)
    return a.lutC > 1 ? launchTmaT<T, GE, 4>(a, tm, s) : launchTmaT<T, GE, 1>(a, tm, s);
 }
 
-bool thermoTmaEligible(const FusedArgs &a, int enc)
+bool tmaRowsAligned(const FusedArgs &a, int enc)
 {
    const int64_t esz = enc == ENC_F32 ? 4 : 8;
-   return a.K > 2 && a.K <= kTmMaxK && a.lutC >= 1 && a.sx == 1 && a.X >= 32 && a.Y >= 9 && a.Z >= 2 &&
-          ((uintptr_t)a.f % 16) == 0 && (a.sy * esz) % 16 == 0 && (a.sz * esz) % 16 == 0 && a.sy >= a.X &&
-          a.sz >= a.sy * a.Y && a.D >= 1 && a.D <= kTmMaxDepth && encodeFn() != nullptr;
+   return a.K > 2 && a.K <= kTmMaxK && a.sx == 1 && a.X >= 32 && a.Y >= 9 && a.Z >= 2 && ((uintptr_t)a.f % 16) == 0 &&
+          (a.sy * esz) % 16 == 0 && (a.sz * esz) % 16 == 0 && a.sy >= a.X && a.sz >= a.sy * a.Y && encodeFn() != nullptr;
+}
+
+bool thermoTmaEligible(const FusedArgs &a, int enc)
+{
+   return tmaRowsAligned(a, enc) && a.lutC >= 1 && a.D >= 1 && a.D <= kTmMaxDepth;
 }
 
 // a.tkey / a.lutC filled (prepareKeys) and the item grid set for 8-row items (itemGrid).
