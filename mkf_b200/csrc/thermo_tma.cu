@@ -130,7 +130,12 @@ __device__ __noinline__ uint32_t exactRankAt(const T *p, const double *sTlo, con
 
 // Word offset of a code held in the top byte of c (bits below masked off), added to base: one
 // multiply-high with an addend.
-__device__ __forceinline__ uint32_t codeAddr(uint32_t c, uint32_t base) { return __umulhi(c, 1024u) + base; }
+__device__ __forceinline__ uint32_t codeAddr(uint32_t c, uint32_t base)
+{
+   uint32_t a;  // (the FMA pipe: the integer ALU pipe is the busier one)
+   asm("mad.hi.u32 %0, %1, 1024, %2;" : "=r"(a) : "r"(c), "r"(base));
+   return a;
+}
 
 // Count the queued wide cells (spread >= 4) of a warp: lane i takes entries i, i + 32, ...; an
 // entry is the cell's two faces of corner ranks (bytes), its smallest rank and spread follow from
