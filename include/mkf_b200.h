@@ -180,19 +180,26 @@ int mkfServerStats(MKFServer *server, MKFServerStats *stats, int reset);
 int mkfServerDestroy(MKFServer *server);
 
 /* ---- tuning (no original counterpart) ----
- * The slab depth of a kernel (planes of cells per work item) trades halo re-reads against work
- * items per SM. mkfTune times the candidate depths on this field with these thresholds (the
- * counting runs several times; synchronous) and keeps the fastest for fields of the same kind:
- * kernel, element type, threshold count and the power-of-two size class of each extent. Later
- * mkfFieldBPFD calls on such fields use it; without tuning each kernel uses its default.
+ * Two launch parameters are chosen per kind of field: the slab depth (planes of cells per work
+ * item: halo re-reads against work items per SM) and, for the TMA-staged rank-table kernel, a
+ * variant of CTA shape and histogram privatisation (0: 20 warps per CTA, two-stage FP64 tile rings,
+ * two histogram copies; 1: 16 warps, three stages, two copies; 2: 20 warps, two stages, one copy).
+ * A kind of field is the kernel, the element type, the threshold count and the power-of-two size
+ * class of each extent (so the row width class too).
+ * mkfTune times the candidate depths (and variants) on this field with these thresholds (the
+ * counting runs several times; synchronous) and keeps the fastest for fields of the same kind;
+ * later mkfFieldBPFD calls on such fields use it; without tuning each kernel uses its default.
  * mkfSetTuning(0 / 1) switches the tuning of new batch plans off / on (default on); it returns
  * the previous setting. */
 int mkfTune(const MKFFieldDesc *pF, const MKFThreshSet *pT, void *stream);
 int mkfSetTuning(int batchPlans);
-/* Record `depth` (1..255 planes) as the slab depth of fields of this kind, as mkfTune records the
- * depth it measured best (for instance one measured in an earlier process); depth 0 forgets the
- * entry. Counts the field once to learn which kernels it takes (synchronous). */
-int mkfTuneSet(const MKFFieldDesc *pF, const MKFThreshSet *pT, int depth, void *stream);
+/* Record `depth` (1..255 planes) and `variant` as the choice for fields of this kind, as mkfTune
+ * records what it measured best (for instance a choice measured in an earlier process); depth 0
+ * forgets the entry. Counts the field once to learn which kernels it takes (synchronous). */
+int mkfTuneSet(const MKFFieldDesc *pF, const MKFThreshSet *pT, int depth, int variant, void *stream);
+/* The depth and variant recorded for this field's kind (0 and 0 when none is). Counts the field
+ * once to learn which kernels it takes (synchronous). */
+int mkfTuneQuery(const MKFFieldDesc *pF, const MKFThreshSet *pT, int *depth, int *variant, void *stream);
 
 /* ---- kernel waits (no original counterpart) ----
  * The kernels that wait on their own asynchronous copies give every wait a limit; a wait that

@@ -20,7 +20,7 @@ from ._lib import (BMC_AL, BMC_EQ, BMC_GT, BMC_LT, ENC_F32, ENC_F64, MKF_F_ACCUM
                    MKFServerStats, MKFThreshSet, check, lib)
 
 __all__ = [
-    "build", "lib", "MKFError", "BatchPlan", "Server", "relation_mask", "field_bpfd", "field_bpfd_moments", "field_bpfd_host", "tune", "set_batch_tuning", "batch_bpfd",
+    "build", "lib", "MKFError", "BatchPlan", "Server", "relation_mask", "field_bpfd", "field_bpfd_moments", "field_bpfd_host", "tune", "tuned", "set_batch_tuning", "batch_bpfd",
     "bin_map_cuda", "get_bpfd", "get_bpfd_host", "measures", "measures_dev", "select_measures",
     "ENC_F32", "ENC_F64", "BMC_LT", "BMC_EQ", "BMC_GT", "BMC_AL",
 ]
@@ -127,17 +127,28 @@ def field_bpfd_moments(field, thresholds, mask=BMC_GT, stream=None):
     return out, mom
 
 
-def tune(field, thresholds, mask=BMC_GT, stream=None, depth=None) -> None:
-    """mkfTune: time the candidate slab depths on this CUDA field and keep the fastest for fields
-    of the same kind (synchronous; the counts of later calls do not change, only their speed).
-    With `depth`, mkfTuneSet: record that depth for such fields instead (0 forgets the entry)."""
+def tune(field, thresholds, mask=BMC_GT, stream=None, depth=None, variant=0) -> None:
+    """mkfTune: time the candidate slab depths (and kernel variants) on this CUDA field and keep the
+    fastest for fields of the same kind (synchronous; the counts of later calls do not change, only
+    their speed). With `depth`, mkfTuneSet: record that depth and `variant` for such fields instead
+    (depth 0 forgets the entry)."""
     th = _Thresholds(thresholds, mask)
     strides = None if field.is_contiguous() else field.stride()
     d = _field_desc(field.data_ptr(), _enc_of(field), field.shape, strides)
     if depth is not None:
-        check(lib().mkfTuneSet(C.byref(d), C.byref(th.ts), int(depth), _stream_ptr(stream)), "mkfTuneSet")
+        check(lib().mkfTuneSet(C.byref(d), C.byref(th.ts), int(depth), int(variant), _stream_ptr(stream)), "mkfTuneSet")
         return
     check(lib().mkfTune(C.byref(d), C.byref(th.ts), _stream_ptr(stream)), "mkfTune")
+
+
+def tuned(field, thresholds, mask=BMC_GT, stream=None):
+    """mkfTuneQuery: (depth, variant) recorded for this field's kind, (0, 0) when none is."""
+    th = _Thresholds(thresholds, mask)
+    strides = None if field.is_contiguous() else field.stride()
+    d = _field_desc(field.data_ptr(), _enc_of(field), field.shape, strides)
+    dep, var = C.c_int(), C.c_int()
+    check(lib().mkfTuneQuery(C.byref(d), C.byref(th.ts), C.byref(dep), C.byref(var), _stream_ptr(stream)), "mkfTuneQuery")
+    return dep.value, var.value
 
 
 def set_batch_tuning(on: bool) -> bool:

@@ -132,7 +132,8 @@ _SIG = [
     ("mkfTune", C.c_int, [C.POINTER(MKFFieldDesc), C.POINTER(MKFThreshSet), _P]),
     ("mkfSetTuning", C.c_int, [C.c_int]),
     ("mkfKernelFaults", C.c_int, [C.c_int]),
-    ("mkfTuneSet", C.c_int, [C.POINTER(MKFFieldDesc), C.POINTER(MKFThreshSet), C.c_int, _P]),
+    ("mkfTuneSet", C.c_int, [C.POINTER(MKFFieldDesc), C.POINTER(MKFThreshSet), C.c_int, C.c_int, _P]),
+    ("mkfTuneQuery", C.c_int, [C.POINTER(MKFFieldDesc), C.POINTER(MKFThreshSet), C.POINTER(C.c_int), C.POINTER(C.c_int), _P]),
     ("mkfServerCreate", C.c_int, [C.POINTER(C.c_void_p), C.POINTER(MKFServerConfig)]),
     ("mkfServerSubmit", C.c_int, [_P, C.POINTER(MKFRequest), C.POINTER(C.c_uint64)]),
     ("mkfServerWait", C.c_int, [_P, C.c_uint64, C.c_double, C.POINTER(C.c_void_p), C.POINTER(C.c_double)]),

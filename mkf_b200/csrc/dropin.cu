@@ -39,13 +39,13 @@ struct PackArgs
 };
 
 // One warp per row (y, z) of the map: lane j thresholds element x = 32 w + j (the sum of the
-// fields) of word w, four words per step with their loads issued together, and a ballot
-// assembles each word; lanes 0..3 store the step's words. Loads are coalesced along x for planar
-// fields; elements past the row end are not read (their bits are 0).
-template <typename T>
+// fields) of word w, U words per step with all their loads issued before the first ballot (U = 8:
+// a 256-element row in one step, 1-2 KB in flight per warp), and a ballot assembles each word;
+// lanes 0..U-1 store the step's words. Loads are coalesced along x for planar fields; elements
+// past the row end are not read (their bits are 0).
+template <typename T, int U>
 __global__ void __launch_bounds__(256) packMap(const __grid_constant__ PackArgs a)
 {
-   constexpr int U = 4;
    const int lane = threadIdx.x & 31;
    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
@@ -53,8 +53,9 @@ __global__ void __launch_bounds__(256) packMap(const __grid_constant__ PackArgs 
    const T t = (T)a.t;
    const T *f0 = (const T *)a.f[0];
    for (long long row = gw; row < nRows; row += nw) {
-      const int z = (int)(row / a.Y);
-      const int y = (int)(row - (long long)z * a.Y);
+      const uint32_t r32 = (uint32_t)row;  // rows fit 32 bits (checked at launch)
+      const int z = (int)(r32 / (uint32_t)a.Y);
+      const int y = (int)(r32 - (uint32_t)z * (uint32_t)a.Y);
       const long long base = (long long)y * a.sy + (long long)z * a.sz;
       uint32_t *wrow = a.w + (size_t)z * a.planeWS + (size_t)y * a.rowWS;
       for (int w0 = 0; w0 < (int)a.rowWS; w0 += U) {
@@ -84,6 +85,52 @@ __global__ void __launch_bounds__(256) packMap(const __grid_constant__ PackArgs 
    }
 }
 
+// One planar field whose rows are whole words (X a multiple of 32): map word i is elements
+// 32 i .. 32 i + 31 of the field, so the map is a flat pass with no row arithmetic. A warp takes 32
+// consecutive words per step: lane j loads element j of each (32 coalesced loads in flight), one
+// ballot per word, and lane i stores word i of the step (one coalesced 128-byte store).
+template <typename T>
+__global__ void __launch_bounds__(256) packFlat(const __grid_constant__ PackArgs a)
+{
+   const int lane = threadIdx.x & 31;
+   const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+   const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+   const T t = (T)a.t;
+   const T *__restrict__ f0 = (const T *)a.f[0];
+   for (long long w0 = gw * 32; w0 < a.nWords; w0 += nw * 32) {
+      const int n = (int)min(32LL, a.nWords - w0);
+      const T *p = f0 + w0 * 32 + lane;
+      T v[32];
+#pragma unroll
+      for (int u = 0; u < 32; u++) { v[u] = u < n ? __ldg(p + 32 * u) : T(0); }
+      uint32_t mine = 0;
+#pragma unroll
+      for (int u = 0; u < 32; u++) {
+         const uint32_t word = __ballot_sync(FULL, (a.m >> relIdx(v[u], t)) & 1u);
+         mine = (lane == u) ? word : mine;
+      }
+      if (lane < n) { a.w[w0 + lane] = mine; }
+   }
+}
+
+template <typename T>
+static void launchPack(const PackArgs &a, long long grid)
+{
+   if (a.nF == 1 && a.sx == 1 && a.sy == a.X && a.sz == (int64_t)a.X * a.Y && (int64_t)a.rowWS * 32 == a.X &&
+       (int64_t)a.planeWS == (int64_t)a.rowWS * a.Y) {
+      long long g = (a.nWords + 32 * 8 - 1) / (32 * 8);  // 8 warps of 32 words per CTA
+      const long long cap = (long long)smCount() * 8;
+      if (g > cap) { g = cap; }
+      packFlat<T><<<(unsigned)(g < 1 ? 1 : g), 256>>>(a);
+      return;
+   }
+   // words per step: as many as a row has, up to 8
+   if (a.rowWS >= 8) { packMap<T, 8><<<(unsigned)grid, 256>>>(a); }
+   else if (a.rowWS >= 4) { packMap<T, 4><<<(unsigned)grid, 256>>>(a); }
+   else if (a.rowWS >= 2) { packMap<T, 2><<<(unsigned)grid, 256>>>(a); }
+   else { packMap<T, 1><<<(unsigned)grid, 256>>>(a); }
+}
+
 struct CountArgs
 {
    const uint32_t *w;
@@ -98,6 +145,7 @@ struct CountArgs
 // four row words and their successors give eight 32-bit corner masks v0..v7 (bit j = corner i of
 // cell x = 32w + j). Uniform cells (all corners equal) are counted by popcount; only mixed cells
 // form their 8-bit code, counted in a per-warp shared histogram.
+template <typename I>
 __global__ void __launch_bounds__(256) countMap(const __grid_constant__ CountArgs a)
 {
    __shared__ uint32_t sh[8][256];
@@ -108,12 +156,14 @@ __global__ void __launch_bounds__(256) countMap(const __grid_constant__ CountArg
    __syncthreads();
    uint32_t *h = sh[warp];
    unsigned long long n0 = 0, n255 = 0;
-   const long long stride = (long long)gridDim.x * blockDim.x;
-   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.nItems; i += stride) {
-      const long long rp = i / a.rowWS;
-      const int wi = (int)(i - rp * a.rowWS);
-      const int y = (int)(rp % (a.rows - 1));
-      const int z = (int)(rp / (a.rows - 1));
+   // (I: 32-bit index arithmetic when every item index fits, else 64-bit)
+   const I stride = (I)gridDim.x * blockDim.x, rowWS = (I)a.rowWS, rowPairs = (I)(a.rows - 1);
+   for (I i = (I)blockIdx.x * blockDim.x + threadIdx.x; i < (I)a.nItems; i += stride) {
+      const I rp = i / rowWS;
+      const int wi = (int)(i - rp * rowWS);
+      const I zq = rp / rowPairs;
+      const int y = (int)(rp - zq * rowPairs);
+      const int z = (int)zq;
       const int nValid = min(32, a.X - 1 - 32 * wi);
       if (nValid <= 0) { continue; }
       const uint32_t vmask = (nValid >= 32) ? 0xFFFFFFFFu : ((1u << nValid) - 1u);
@@ -169,10 +219,14 @@ static int launchCount(unsigned long long *out, const BMOrg *pO, const uint32_t 
    a.out = out;
    if (pO->rowPairs == 0 || pO->planePairs == 0 || pO->rowElem < 2 || pO->rowWS == 0) { return MKF_OK; }
    a.nItems = (long long)a.rowWS * pO->rowPairs * pO->planePairs;
-   long long grid = (a.nItems + 255) / 256;
-   const long long cap = (long long)smCount() * 8;
+   // at least 4 words per thread, at most 4 CTAs per SM: every CTA ends with up to 256 global
+   // atomics on the same 256 counters, so fewer, busier CTAs finish sooner
+   long long grid = (a.nItems + 1023) / 1024;
+   const long long cap = (long long)smCount() * 4;
    if (grid > cap) { grid = cap; }
-   countMap<<<(unsigned)grid, 256, 0, s>>>(a);
+   if (grid < 1) { grid = 1; }
+   if (a.nItems + grid * 256 < (1LL << 31)) { countMap<uint32_t><<<(unsigned)grid, 256, 0, s>>>(a); }
+   else { countMap<unsigned long long><<<(unsigned)grid, 256, 0, s>>>(a); }
    return cudaFail(cudaGetLastError(), "countMap launch");
 }
 
@@ -257,12 +311,16 @@ MKF_API BMPackWord *binMapCUDA(KernInfo *pK, BMPackWord *pW, BMOrg *pO, const BM
    a.m = pM->m;
    a.w = pW;
    a.nWords = (long long)org.rowWS * a.Y * a.Z;
+   if ((long long)a.Y * a.Z >= (1LL << 32)) {
+      logError("binMapCUDA() - %d x %d rows exceed 2^32\n", a.Y, a.Z);
+      return nullptr;
+   }
    EventTimer tm;
    long long grid = ((long long)a.Y * a.Z + 7) / 8;  // a warp per row
-   const long long cap = (long long)smCount() * 16;
+   const long long cap = (long long)smCount() * 8;      // one wave of 8 CTAs (64 warps) per SM
    if (grid > cap) { grid = cap; }
-   if (pF->elemID == ENC_F32) { packMap<float><<<(unsigned)grid, 256>>>(a); }
-   else { packMap<double><<<(unsigned)grid, 256>>>(a); }
+   if (pF->elemID == ENC_F32) { launchPack<float>(a, grid); }
+   else { launchPack<double>(a, grid); }
    cudaError_t e = cudaGetLastError();
    const float ms = tm.stop();
    if (e == cudaSuccess) { e = cudaGetLastError(); }

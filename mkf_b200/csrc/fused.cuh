@@ -110,6 +110,9 @@ int planBatchField(const MKFFieldDesc *pF, const MKFThreshSet *pT, int rowBase, 
 // (tune.cu): the depth mkfTune measured best for this kind of field, else `def`.
 enum { kFamWords = 0, kFamThermo = 1, kFamThermoTma = 2 };
 int tunedDepth(int family, int enc, int K, int X, int Y, int Z, int def);
+// Kernel variant (CTA shape, histogram copies) of such a launch: the one mkfTune measured best for
+// this kind of field, else `def`. Families without variants use 0.
+int tunedVariant(int family, int enc, int K, int X, int Y, int Z, int def);
 // The untuned slab depth: def halved (down to 4) until a field of itemsPerPlane work items per
 // plane and Z planes has at least minItems items.
 int sizeDepth(int def, long long itemsPerPlane, int Z, long long minItems);

@@ -467,7 +467,7 @@ int launchThermo(FusedArgs &a, int enc, cudaStream_t s)
    if (thermoTmaEligible(a, enc)) {
       itemGrid(a, tunedDepth(kFamThermoTma, enc, a.K, a.X, a.Y, a.Z,
                              sizeDepth(THERMO_D, perPlane, a.Z, (long long)smCount() * kTmItemsPerSM)));
-      const int rc = launchThermoTma(a, enc, s);
+      const int rc = launchThermoTma(a, enc, tunedVariant(kFamThermoTma, enc, a.K, a.X, a.Y, a.Z, 0), s);
       if (rc != MKF_ERR_UNSUPPORTED) { return rc; }
    }
 #endif

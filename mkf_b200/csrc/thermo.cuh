@@ -215,13 +215,14 @@ __host__ __device__ constexpr size_t thermoDynBytes(int K)
 }
 
 // Load one field's thresholds, build its rank table and clear the histogram (whole CTA).
-// copyRows: histogram rows per copy (K, or more when rows past K take discarded counts).
+// copyRows: histogram rows per copy (K, or more when rows past K take discarded counts);
+// copies: histogram copies.
 template <typename P>
-__device__ void ctaSetup(const P &a, ThermoShared &S, uint32_t *hist, int copyRows = 0)
+__device__ void ctaSetup(const P &a, ThermoShared &S, uint32_t *hist, int copyRows = 0, int copies = kHistCopies)
 {
    const int K = a.K;
    const int rows = copyRows > 0 ? copyRows : K;
-   for (int i = threadIdx.x; i < rows * kHistRow * kHistCopies; i += blockDim.x) { hist[i] = 0; }
+   for (int i = threadIdx.x; i < rows * kHistRow * copies; i += blockDim.x) { hist[i] = 0; }
    for (int i = threadIdx.x; i < 64; i += blockDim.x) {
       S.tlo[i] = a.tlo[i];
       S.thi[i] = a.thi[i];
@@ -254,7 +255,7 @@ __device__ void ctaSetup(const P &a, ThermoShared &S, uint32_t *hist, int copyRo
 // Add the CTA's counts of one field to its output rows (whole CTA; call after every warp has
 // added its cells to S.cells): mixed codes as counted, 255 from the all-ones sums, 0 = the rest.
 template <typename P>
-__device__ void ctaFlush(const P &a, ThermoShared &S, const uint32_t *hist, int copyRows = 0)
+__device__ void ctaFlush(const P &a, ThermoShared &S, const uint32_t *hist, int copyRows = 0, int copies = kHistCopies)
 {
    __syncthreads();
    const int K = a.K;
@@ -263,8 +264,7 @@ __device__ void ctaFlush(const P &a, ThermoShared &S, const uint32_t *hist, int 
    for (int k = warp; k < K; k += nWarps) {
       uint32_t s = 0;
       for (int c = 1 + lane; c < 255; c += 32) {
-#pragma unroll
-         for (int q = 0; q < kHistCopies; ++q) { s += hist[(q * rows + k) * kHistRow + c]; }
+         for (int q = 0; q < copies; ++q) { s += hist[(q * rows + k) * kHistRow + c]; }
       }
       s = __reduce_add_sync(FULL, s);
       if (lane == 0) {
@@ -279,8 +279,7 @@ __device__ void ctaFlush(const P &a, ThermoShared &S, const uint32_t *hist, int 
    for (int i = threadIdx.x; i < K * 256; i += blockDim.x) {
       const int c = i & 255;
       uint32_t v = 0;
-#pragma unroll
-      for (int q = 0; q < kHistCopies; ++q) { v += hist[(q * rows + (i >> 8)) * kHistRow + c]; }
+      for (int q = 0; q < copies; ++q) { v += hist[(q * rows + (i >> 8)) * kHistRow + c]; }
       if (v && c != 0 && c != 255) {
          const int cc = a.complement ? 255 - c : c;
          atomicAdd((unsigned long long *)(a.out + (size_t)a.outRow[i >> 8] * 256 + cc), (unsigned long long)v);
@@ -328,6 +327,8 @@ __device__ __forceinline__ uint32_t cellCode(uint32_t R0, uint32_t R1, uint32_t 
 // and itemGrid), and its launch (MKF_ERR_UNSUPPORTED when it does not take it).
 static constexpr int kTmItemsPerSM = 80;  // four items per resident warp (20 per SM)
 bool thermoTmaEligible(const FusedArgs &a, int enc);
-int launchThermoTma(const FusedArgs &a, int enc, cudaStream_t s);
+// variant: CTA shape and histogram privatisation (kTmVariants in thermo_tma.cu), 0 = default.
+static constexpr int kTmNumVariants = 3;
+int launchThermoTma(const FusedArgs &a, int enc, int variant, cudaStream_t s);
 
 }  // namespace mkf

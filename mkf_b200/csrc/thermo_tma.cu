@@ -37,16 +37,14 @@
 
 namespace mkf {
 
-#ifndef TMA_WARPS
-#define TMA_WARPS 20
-#endif
-#ifndef TMA_STAGES_F64
-#define TMA_STAGES_F64 2
-#endif
-#ifndef TMA_STAGES_F32
-#define TMA_STAGES_F32 3
-#endif
-static constexpr int kTmWarps = TMA_WARPS;
+// Kernel variants (the CTA shape and the histogram privatisation mkfTune chooses among; 0 is the
+// default): warps per CTA (one CTA per SM), ring stages for FP64 / FP32 tiles, histogram copies
+// (lane parity picks the copy; one copy halves that shared memory).
+struct TmaVariant
+{
+   int warps, stagesF64, stagesF32, copies;
+};
+static constexpr TmaVariant kTmVariants[kTmNumVariants] = {{20, 2, 3, 2}, {16, 3, 4, 2}, {20, 2, 3, 1}};
 static constexpr int kTmRows = 9;           // rows of a plane tile: 8 row pairs
 // wide-cell queue entries per warp: a plane adds at most 8 x 31, drained once 32 are waiting (plus
 // one discard entry)
@@ -55,14 +53,16 @@ static constexpr int kTmMaxK = 16;          // thresholds a 16-bit thermometer h
 static constexpr long kTmWaitLimit = 1L << 22;  // mbarrier polls before a wait gives up
 static constexpr int kTmMaxDepth = kThMaxDepth;  // planes per work item
 
-// Element type geometry: tile width (x positions, a multiple of 16 bytes that covers 32 lanes
-// plus the alignment shift of the tile's first x), stages in the ring, bytes per stage.
-template <typename T>
+// Element type and variant geometry: tile width (x positions, a multiple of 16 bytes that covers
+// 32 lanes plus the alignment shift of the tile's first x), stages in the ring, bytes per stage.
+template <typename T, int V = 0>
 struct TmaGeom
 {
    static constexpr int BX = sizeof(T) == 8 ? 34 : 36;
    static constexpr int ALIGN = 16 / (int)sizeof(T);  // x coordinates of a TMA tile: multiples of this
-   static constexpr int STAGES = sizeof(T) == 8 ? TMA_STAGES_F64 : TMA_STAGES_F32;
+   static constexpr int WARPS = kTmVariants[V].warps;
+   static constexpr int STAGES = sizeof(T) == 8 ? kTmVariants[V].stagesF64 : kTmVariants[V].stagesF32;
+   static constexpr int COPIES = kTmVariants[V].copies;
    static constexpr int BYTES = BX * kTmRows * (int)sizeof(T);   // bytes one TMA copy writes
    static constexpr int PITCH = (BYTES + 127) / 128 * 128;       // stage stride
 };
@@ -230,11 +230,12 @@ __device__ __forceinline__ TmItem itemOf(const FusedArgs &a, long long it, int l
    return m;
 }
 
-template <typename T, bool GE, int CMAX>
-__global__ void __launch_bounds__(kTmWarps * 32, 1)
+template <typename T, bool GE, int CMAX, int V>
+__global__ void __launch_bounds__(kTmVariants[V].warps * 32, 1)
     thermoTmaBPFD(const __grid_constant__ FusedArgs a, const __grid_constant__ CUtensorMap tm)
 {
-   using G = TmaGeom<T>;
+   using G = TmaGeom<T, V>;
+   constexpr int kTmWarps = G::WARPS, kHistCopies = G::COPIES;
    constexpr int W = sizeof(T) / 4;   // 32-bit words per element; the ranked word is the last
    constexpr int S = G::STAGES;
    __shared__ ThermoShared Sh;
@@ -256,7 +257,7 @@ __global__ void __launch_bounds__(kTmWarps * 32, 1)
       for (int s = 0; s < S; s++) { mbarInit((uint32_t)__cvta_generic_to_shared(&bars[warp][s]), 1); }
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
    }
-   ctaSetup(a, Sh, hist, copyRows);  // (its barriers also order the mbarrier set-up)
+   ctaSetup(a, Sh, hist, copyRows, kHistCopies);  // (its barriers also order the mbarrier set-up)
 
    const uint32_t ringW = (uint32_t)__cvta_generic_to_shared(ring) + (uint32_t)(warp * S * G::PITCH);
    const uint32_t bar0 = (uint32_t)__cvta_generic_to_shared(&bars[warp][0]);
@@ -455,17 +456,17 @@ __global__ void __launch_bounds__(kTmWarps * 32, 1)
          above += nr[k];
       }
    }
-   ctaFlush(a, Sh, hist, copyRows);
+   ctaFlush(a, Sh, hist, copyRows, kHistCopies);
 }
 
 // ---------------------------------------------------------------- host
 
-template <typename T>
+template <typename T, int V>
 static size_t tmaDynBytes(int K)
 {
-   using G = TmaGeom<T>;
-   const size_t histBytes = ((size_t)tmaCopyRows(K) * kHistRow * kHistCopies * 4 + 127) / 128 * 128;
-   return histBytes + 128 + (size_t)kTmWarps * G::STAGES * G::PITCH + (size_t)kTmWarps * (kTmQueue + 1) * sizeof(uint2);
+   using G = TmaGeom<T, V>;
+   const size_t histBytes = ((size_t)tmaCopyRows(K) * kHistRow * G::COPIES * 4 + 127) / 128 * 128;
+   return histBytes + 128 + (size_t)G::WARPS * G::STAGES * G::PITCH + (size_t)G::WARPS * (kTmQueue + 1) * sizeof(uint2);
 }
 
 static PFN_cuTensorMapEncodeTiled_v12000 encodeFn()
@@ -485,25 +486,32 @@ static PFN_cuTensorMapEncodeTiled_v12000 encodeFn()
    return fn;
 }
 
-template <typename T, bool GE, int CMAX>
+template <typename T, bool GE, int CMAX, int V>
 static int launchTmaT(const FusedArgs &a, const CUtensorMap &tm, cudaStream_t s)
 {
+   using G = TmaGeom<T, V>;
    static std::atomic<int> occ[kTmMaxK + 1];
-   auto kern = thermoTmaBPFD<T, GE, CMAX>;
-   const size_t smem = tmaDynBytes<T>(a.K);
-   const int blocksPerSM = cachedOccupancy(occ[a.K], kern, kTmWarps * 32, smem, tmaDynBytes<T>(kTmMaxK));
-   long long grid = (a.nItems + kTmWarps - 1) / kTmWarps;
+   auto kern = thermoTmaBPFD<T, GE, CMAX, V>;
+   const size_t smem = tmaDynBytes<T, V>(a.K);
+   const int blocksPerSM = cachedOccupancy(occ[a.K], kern, G::WARPS * 32, smem, tmaDynBytes<T, V>(kTmMaxK));
+   long long grid = (a.nItems + G::WARPS - 1) / G::WARPS;
    const long long cap = (long long)smCount() * blocksPerSM;
    if (grid > cap) { grid = cap; }
    if (grid < 1) { grid = 1; }
-   kern<<<(unsigned)grid, kTmWarps * 32, smem, s>>>(a, tm);
+   kern<<<(unsigned)grid, G::WARPS * 32, smem, s>>>(a, tm);
    return cudaFail(cudaGetLastError(), "thermoTmaBPFD launch");
 }
 
+// Thresholds sharing rank-table buckets (four candidates) take the default variant only.
 template <typename T, bool GE>
-static int launchTmaG(const FusedArgs &a, const CUtensorMap &tm, cudaStream_t s)
+static int launchTmaG(const FusedArgs &a, const CUtensorMap &tm, int variant, cudaStream_t s)
 {
-   return a.lutC > 1 ? launchTmaT<T, GE, 4>(a, tm, s) : launchTmaT<T, GE, 1>(a, tm, s);
+   if (a.lutC > 1) { return launchTmaT<T, GE, 4, 0>(a, tm, s); }
+   switch (variant) {
+      case 1: return launchTmaT<T, GE, 1, 1>(a, tm, s);
+      case 2: return launchTmaT<T, GE, 1, 2>(a, tm, s);
+      default: return launchTmaT<T, GE, 1, 0>(a, tm, s);
+   }
 }
 
 bool tmaRowsAligned(const FusedArgs &a, int enc)
@@ -519,7 +527,7 @@ bool thermoTmaEligible(const FusedArgs &a, int enc)
 }
 
 // a.tkey / a.lutC filled (prepareKeys) and the item grid set for 8-row items (itemGrid).
-int launchThermoTma(const FusedArgs &a, int enc, cudaStream_t s)
+int launchThermoTma(const FusedArgs &a, int enc, int variant, cudaStream_t s)
 {
    if (!thermoTmaEligible(a, enc)) { return MKF_ERR_UNSUPPORTED; }
    const bool f32 = enc == ENC_F32;
@@ -535,8 +543,8 @@ int launchThermoTma(const FusedArgs &a, int enc, cudaStream_t s)
                                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
    if (cr != CUDA_SUCCESS) { return MKF_ERR_UNSUPPORTED; }
    const bool ge = a.rankHi != 0;
-   if (f32) { return ge ? launchTmaG<float, true>(a, tm, s) : launchTmaG<float, false>(a, tm, s); }
-   return ge ? launchTmaG<double, true>(a, tm, s) : launchTmaG<double, false>(a, tm, s);
+   if (f32) { return ge ? launchTmaG<float, true>(a, tm, variant, s) : launchTmaG<float, false>(a, tm, variant, s); }
+   return ge ? launchTmaG<double, true>(a, tm, variant, s) : launchTmaG<double, false>(a, tm, variant, s);
 }
 
 }  // namespace mkf

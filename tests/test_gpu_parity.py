@@ -498,6 +498,17 @@ def test_tuning_keeps_counts(mkf, cuda):
         mkf.tune(f, t, 4)
     for (f, t), b in zip(cases, before):
         assert (u64(mkf.field_bpfd(f, t, 4)) == b).all()
+    # the 16-threshold FP64 field takes the TMA-staged rank-table kernel: mkfTune recorded a depth
+    # and one of its variants, and every variant (CTA shape, histogram copies) keeps the counts
+    depth, variant = mkf.tuned(f64, cases[0][1], 4)
+    assert depth in (4, 8, 16, 32, 64, 128) and variant in (0, 1, 2)
+    for v in (0, 1, 2):
+        for dep in (8, 64):
+            mkf.tune(f64, cases[0][1], 4, depth=dep, variant=v)
+            assert mkf.tuned(f64, cases[0][1], 4) == (dep, v)
+            assert (u64(mkf.field_bpfd(f64, cases[0][1], 4)) == before[0]).all(), (v, dep)
+    mkf.tune(f64, cases[0][1], 4, depth=0)
+    assert mkf.tuned(f64, cases[0][1], 4) == (0, 0)
     fields = [f64, f32, f32[:40, :50, :60]]
     ths = [np.linspace(-1.5, 1.5, 16), [0.2], [0.1, 0.3]]
     plans = []
@@ -746,7 +757,8 @@ def test_benchmark_config_equals_reference_c_path(mkf, ref_oracle, cuda):
     bit for bit, as the reference's own test compares its CPU and GPU distributions
     (mkfTest.c:64-85). Slab depths: the untuned default, the depth the benchmark's tuning keeps on
     the 1024^3 field (128 planes: two full work items and a short one along z) and the
-    candidates of mkfTune; every work item is shifted inside the field (X >= 32, Y > 8). The
+    candidates of mkfTune, with the TMA-staged kernel's variants of CTA shape and histogram
+    copies; every work item is shifted inside the field (X >= 32, Y > 8). The
     reference's interface rounds thresholds to float (binMapUtil.c:37), so both sides are given
     the float-rounded thresholds."""
     import torch
@@ -764,11 +776,11 @@ def test_benchmark_config_equals_reference_c_path(mkf, ref_oracle, cuda):
     want = np.stack([ref_oracle.bpfd_mt(host, (1024, 1024, Z), float(tv), mkf.BMC_GT, threads) for tv in t])
     assert (want.sum(axis=1) == 1023 * 1023 * (Z - 1)).all()
     del host
-    for depth in (None, 128, 64, 32, 8, 4):
+    for depth, variant in ((None, 0), (128, 0), (64, 0), (32, 0), (8, 0), (4, 0), (128, 1), (64, 2)):
         if depth is not None:
-            mkf.tune(f, t, mkf.BMC_GT, depth=depth)
+            mkf.tune(f, t, mkf.BMC_GT, depth=depth, variant=variant)
         got = u64(mkf.field_bpfd(f, t, mkf.BMC_GT))
-        assert (got == want).all(), depth
+        assert (got == want).all(), (depth, variant)
     mkf.tune(f, t, mkf.BMC_GT)
     assert (u64(mkf.field_bpfd(f, t, mkf.BMC_GT)) == want).all()
     mkf.tune(f, t, mkf.BMC_GT, depth=0)
