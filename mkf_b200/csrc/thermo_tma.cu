@@ -34,6 +34,7 @@
 #include <cstring>
 #include <mutex>
 #include "thermo.cuh"
+#include "tma.cuh"
 
 namespace mkf {
 
@@ -50,7 +51,6 @@ static constexpr int kTmRows = 9;           // rows of a plane tile: 8 row pairs
 // one discard entry)
 static constexpr int kTmQueue = 32 + 8 * 31;  // drained after a plane once 32 are waiting
 static constexpr int kTmMaxK = 16;          // thresholds a 16-bit thermometer holds
-static constexpr long kTmWaitLimit = 1L << 22;  // mbarrier polls before a wait gives up
 static constexpr int kTmMaxDepth = kThMaxDepth;  // planes per work item
 
 // Element type and variant geometry: tile width (x positions, a multiple of 16 bytes that covers
@@ -69,40 +69,6 @@ struct TmaGeom
 
 // Set when a wait of this kernel ran out of polls (never in a correct run); read by mkfKernelFaults.
 __device__ unsigned gTmaFault;
-
-__device__ __forceinline__ void mbarInit(uint32_t bar, uint32_t count)
-{
-   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-
-// Lane 0: announce the bytes of the next phase and start the copy of one plane tile.
-__device__ __forceinline__ void tmaPlane(const CUtensorMap *tm, uint32_t dst, uint32_t bar, int x, int y, int z,
-                                         uint32_t bytes)
-{
-   // the stage was last read through the generic proxy; order those reads before the async write
-   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-   asm volatile(
-       "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
-       "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(z), "r"(bar)
-       : "memory");
-}
-
-// Wait for phase `parity` of a barrier; false after kTmWaitLimit polls.
-__device__ __forceinline__ bool mbarWait(uint32_t bar, uint32_t parity)
-{
-   for (long i = 0; i < kTmWaitLimit; i++) {
-      uint32_t done;
-      asm volatile(
-          "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
-          : "=r"(done)
-          : "r"(bar), "r"(parity)
-          : "memory");
-      if (done) { return true; }
-   }
-   return false;
-}
-
 
 // Histogram rows per copy: K real rows, then discard rows up to max(K, 16) + 2, where the slots
 // of cells that cross fewer than three thresholds (and of masked cells, whose low half is 16 set
@@ -280,7 +246,7 @@ __global__ void __launch_bounds__(kTmVariants[V].warps * 32, 1)
       if (pIt >= a.nItems) { return; }
       if (lane == 0) {
          const uint32_t st = gp % S;
-         tmaPlane(&tm, ringW + st * G::PITCH, bar0 + 8u * st, pX, pY, pZ + pP, G::BYTES);
+         tmaTile3D(&tm, ringW + st * G::PITCH, bar0 + 8u * st, pX, pY, pZ + pP, G::BYTES);
       }
       ++gp;
       if (++pP > pN) {
@@ -486,6 +452,34 @@ static PFN_cuTensorMapEncodeTiled_v12000 encodeFn()
    return fn;
 }
 
+bool encodeField3D(CUtensorMap *tm, const void *base, int enc, int X, int Y, int Z, int64_t sy, int64_t sz, int boxX, int boxY,
+                   bool promote256)
+{
+   const cuuint64_t esz = enc == ENC_F32 ? 4 : 8;
+   if (!encodeFn() || ((uintptr_t)base % 16) != 0 || (sy * (int64_t)esz) % 16 != 0 || (sz * (int64_t)esz) % 16 != 0) {
+      return false;
+   }
+   const cuuint64_t dims[3] = {(cuuint64_t)X, (cuuint64_t)Y, (cuuint64_t)Z};
+   const cuuint64_t strides[2] = {(cuuint64_t)sy * esz, (cuuint64_t)sz * esz};
+   const cuuint32_t box[3] = {(cuuint32_t)boxX, (cuuint32_t)boxY, 1};
+   const cuuint32_t estr[3] = {1, 1, 1};
+   return encodeFn()(tm, enc == ENC_F32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+                     const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_NONE, promote256 ? CU_TENSOR_MAP_L2_PROMOTION_L2_256B : CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+unsigned thermoTmaFaults(bool clear)
+{
+   unsigned v = 0;
+   if (cudaMemcpyFromSymbol(&v, gTmaFault, sizeof(v)) != cudaSuccess) { cudaGetLastError(); return 0; }
+   if (clear && v) {
+      const unsigned z = 0;
+      cudaMemcpyToSymbol(gTmaFault, &z, sizeof(z));
+   }
+   return v;
+}
+
 template <typename T, bool GE, int CMAX, int V>
 static int launchTmaT(const FusedArgs &a, const CUtensorMap &tm, cudaStream_t s)
 {
@@ -531,17 +525,10 @@ int launchThermoTma(const FusedArgs &a, int enc, int variant, cudaStream_t s)
 {
    if (!thermoTmaEligible(a, enc)) { return MKF_ERR_UNSUPPORTED; }
    const bool f32 = enc == ENC_F32;
-   const cuuint64_t esz = f32 ? 4 : 8;
    CUtensorMap tm;
-   const cuuint64_t dims[3] = {(cuuint64_t)a.X, (cuuint64_t)a.Y, (cuuint64_t)a.Z};
-   const cuuint64_t strides[2] = {(cuuint64_t)a.sy * esz, (cuuint64_t)a.sz * esz};
-   const cuuint32_t box[3] = {(cuuint32_t)(f32 ? TmaGeom<float>::BX : TmaGeom<double>::BX), (cuuint32_t)kTmRows, 1};
-   const cuuint32_t estr[3] = {1, 1, 1};
-   const CUresult cr = encodeFn()(&tm, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
-                                  const_cast<void *>(a.f), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-   if (cr != CUDA_SUCCESS) { return MKF_ERR_UNSUPPORTED; }
+   if (!encodeField3D(&tm, a.f, enc, a.X, a.Y, a.Z, a.sy, a.sz, f32 ? TmaGeom<float>::BX : TmaGeom<double>::BX, kTmRows)) {
+      return MKF_ERR_UNSUPPORTED;
+   }
    const bool ge = a.rankHi != 0;
    if (f32) { return ge ? launchTmaG<float, true>(a, tm, variant, s) : launchTmaG<float, false>(a, tm, variant, s); }
    return ge ? launchTmaG<double, true>(a, tm, variant, s) : launchTmaG<double, false>(a, tm, variant, s);
@@ -551,13 +538,6 @@ int launchThermoTma(const FusedArgs &a, int enc, int variant, cudaStream_t s)
 
 MKF_API int mkfKernelFaults(int clear)
 {
-   unsigned v = 0;
-   cudaError_t e = cudaMemcpyFromSymbol(&v, mkf::gTmaFault, sizeof(v));
-   if (e != cudaSuccess) { return mkf::cudaFail(e, "mkfKernelFaults"); }
-   if (clear && v) {
-      const unsigned z = 0;
-      e = cudaMemcpyToSymbol(mkf::gTmaFault, &z, sizeof(z));
-      if (e != cudaSuccess) { return mkf::cudaFail(e, "mkfKernelFaults"); }
-   }
+   const unsigned v = mkf::thermoTmaFaults(clear != 0);
    return (int)v;
 }

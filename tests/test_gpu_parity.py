@@ -861,3 +861,4 @@ def test_tma_rank_table_kernel_exact_path_and_depths(mkf, oracle, cuda, dtype):
         assert (u64(mkf.field_bpfd(fd, t, mkf.BMC_GT)) == want).all(), depth
     mkf.tune(fd, t, mkf.BMC_GT, depth=0)
     assert mkf.lib().mkfKernelFaults(1) == 0
+
