@@ -214,10 +214,11 @@ def run_batch_workload(dev, n_fields=512, seed=SEED + 3, reps=3):
     return res
 
 
-def serving_pool(dev, n=48, seed=SEED + 4):
-    """Fields a serving run draws from: voxel counts log-uniform in [32^3, 512^3], aspect ratios up
-    to 4:1, 70 % FP32 / 30 % FP64, ball content; even entries stay on the device, odd ones are
-    pinned host copies (the server stages those)."""
+def serving_pool(dev, n=256, seed=SEED + 4):
+    """Distinct fields a serving run draws from (requests cycle through them in a shuffled order,
+    so no field repeats within n requests): voxel counts log-uniform in [32^3, 512^3], aspect
+    ratios up to 4:1, 70 % FP32 / 30 % FP64, ball content; even entries stay on the device, odd
+    ones are pinned host copies (the server stages those). 256 fields hold about 20 GB."""
     import torch
 
     rng = np.random.default_rng(seed)
@@ -337,10 +338,12 @@ def run_plain_workload(dev, steps=20, warmup=5):
 def run_serving_workload(dev, rates=(100, 500, 1000, 2000, 5000), max_requests=10000, seconds=3.0,
                          seed=SEED + 5):
     """Poisson request streams at each rate (min(10000, rate x 3 s) requests, so every rate runs a
-    few seconds): each request takes a random pool field and 1-8 thresholds in [-2, 2] (relation
-    >), counts stay on the device until the client has waited for them and released them. Reports
-    p50/p99 latency (submission to completion) and throughput per rate, the saturated throughput
-    (every request submitted at once), and the plain per-field drop-in call on the same mix."""
+    few seconds): each request takes the next field of a shuffled cycle through the pool and 1-8
+    thresholds in [-2, 2] (relation >), counts stay on the device until the client has waited for
+    them and released them. Reports p50/p99 latency (submission to completion) and throughput per
+    rate, the saturated throughput (every request submitted at once), the device time of the
+    launches and the worker's host planning time, the same device-resident requests as one batch
+    plan (the kernels alone), and the plain per-field drop-in call on the same mix."""
     import threading
 
     import torch
@@ -351,10 +354,17 @@ def run_serving_workload(dev, rates=(100, 500, 1000, 2000, 5000), max_requests=1
     rng = np.random.default_rng(seed)
     srv = mkf_b200.Server(hbm_budget=64 << 30)
 
+    cursor = [0, rng.permutation(len(pool))]
+
     def requests(n):
-        idx = rng.integers(0, len(pool), size=n)
+        idx = []
+        for _ in range(n):  # a shuffled cycle through the pool: distinct fields within a cycle
+            if cursor[0] == len(pool):
+                cursor[0], cursor[1] = 0, rng.permutation(len(pool))
+            idx.append(int(cursor[1][cursor[0]]))
+            cursor[0] += 1
         ks = rng.integers(1, 9, size=n)
-        return [(int(i), np.sort(rng.uniform(-2, 2, size=int(k)))) for i, k in zip(idx, ks)]
+        return [(i, np.sort(rng.uniform(-2, 2, size=int(k)))) for i, k in zip(idx, ks)]
 
     def stream(reqs, rate):
         gaps = rng.exponential(1.0 / rate, size=len(reqs)) if rate else np.zeros(len(reqs))
@@ -391,13 +401,34 @@ def run_serving_workload(dev, rates=(100, 500, 1000, 2000, 5000), max_requests=1
         return {"requests": len(reqs), "offered_per_s": rate, "fields_per_s": len(reqs) / (t1 - t0),
                 "gvoxel_per_s": vox / (t1 - t0) * 1e-9, "h2d_gb_per_s": h2d / (t1 - t0) * 1e-9,
                 "p50_ms": st["p50"] * 1e3, "p99_ms": st["p99"] * 1e3,
-                "launches": st["launches"], "mean_fields_per_launch": st["meanFieldsInLaunch"]}
+                "launches": st["launches"], "mean_fields_per_launch": st["meanFieldsInLaunch"],
+                "launch_device_s": st["launchDeviceSec"], "plan_host_s": st["planHostSec"], "wall_s": t1 - t0}
 
     stream(requests(200), 0)  # warm-up
     per_rate = [stream(requests(int(min(max_requests, r * seconds))), r) for r in rates]
     burst = stream(requests(2000), 0)
     dev_only = [r for r in requests(6000) if pool[r[0]].is_cuda][:2000]
     burst_dev = stream(dev_only, 0)
+    # the kernels alone on the same device-resident mix: 128 of those requests on distinct fields
+    # as one batch plan, against the server running the same requests
+    head, seen = [], set()
+    for r in dev_only:
+        if r[0] not in seen and len(head) < 128:
+            seen.add(r[0])
+            head.append(r)
+    plan = mkf_b200.BatchPlan([pool[i] for i, _ in head], [t for _, t in head])
+    plan.launch()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(3):
+        plan.launch()
+    e1.record()
+    torch.cuda.synchronize(dev)
+    plan_s = e0.elapsed_time(e1) * 1e-3 / 3
+    plan.close()
+    head_vox = sum(pool[i].numel() for i, _ in head)
+    served_head = stream(head, 0)
 
     # the plain per-field call on a sample of the same mix: host fields copied first, then one
     # binMapCUDA + mkfCUDAGetBPFDH per threshold, as a caller of the original library would
@@ -422,6 +453,13 @@ def run_serving_workload(dev, rates=(100, 500, 1000, 2000, 5000), max_requests=1
         "saturated_device_resident_fields_per_s": burst_dev["fields_per_s"],
         "saturated_device_resident_gvoxel_per_s": burst_dev["gvoxel_per_s"],
         "saturated_device_resident_p99_ms": burst_dev["p99_ms"],
+        "saturated_device_resident_launch_device_s": burst_dev["launch_device_s"],
+        "saturated_device_resident_plan_host_s": burst_dev["plan_host_s"],
+        "saturated_device_resident_wall_s": burst_dev["wall_s"],
+        "device_resident_128_batch_plan_gvoxel_per_s": head_vox / plan_s * 1e-9,
+        "device_resident_128_served_gvoxel_per_s": served_head["gvoxel_per_s"],
+        "device_resident_128_served_launch_device_s": served_head["launch_device_s"],
+        "device_resident_128_served_wall_s": served_head["wall_s"],
         "bound": "host-to-device copies of the pinned-host half of the requests (PCIe) at saturation",
         "saturated_p99_ms": burst["p99_ms"],
         "plain_dropin_fields_per_s": plain,

@@ -160,6 +160,10 @@ typedef struct
    double meanFieldsInLaunch;
    double p50, p99, mean, max;  /* latency in seconds, submission to completion seen by the server */
    uint64_t deviceBytesInUse;   /* budget in use now (staged fields + held counts) */
+   double launchDeviceSec;      /* summed device time of the launches, from the last staged field
+                                 * copied to the last count written (launches on the two launch
+                                 * streams may overlap, so this can exceed wall time) */
+   double planHostSec;          /* host time the worker spent planning and issuing launches */
 } MKFServerStats;
 
 int mkfServerCreate(MKFServer **pServer, const MKFServerConfig *cfg);

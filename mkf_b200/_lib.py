@@ -86,7 +86,7 @@ class MKFServerStats(C.Structure):
     _fields_ = [("completed", C.c_uint64), ("failed", C.c_uint64), ("launches", C.c_uint64),
                 ("maxFieldsInLaunch", C.c_uint32), ("pad_", C.c_uint32), ("meanFieldsInLaunch", C.c_double),
                 ("p50", C.c_double), ("p99", C.c_double), ("mean", C.c_double), ("max", C.c_double),
-                ("deviceBytesInUse", C.c_uint64)]
+                ("deviceBytesInUse", C.c_uint64), ("launchDeviceSec", C.c_double), ("planHostSec", C.c_double)]
 
 
 _SIG = [

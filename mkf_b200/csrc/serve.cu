@@ -93,7 +93,7 @@ struct DevBuf
 struct LaunchSlot
 {
    cudaStream_t stream = nullptr;
-   cudaEvent_t copied = nullptr, done = nullptr;
+   cudaEvent_t copied = nullptr, start = nullptr, done = nullptr;
    std::vector<Request *> reqs;
    DevBuf work;      // tasks, chunks, clear list (uploaded each launch)
    DevBuf results;   // counts of requests that want them on the host
@@ -123,6 +123,7 @@ struct MKFServer
    // statistics (under mu)
    std::vector<double> latency;
    uint64_t launches = 0, failed = 0, fieldsLaunched = 0;
+   double launchDeviceSec = 0.0, planHostSec = 0.0;
    uint32_t maxInLaunch = 0;
    std::string fatal;
 };
@@ -156,6 +157,7 @@ static int issueLaunch(MKFServer *s, LaunchSlot &sl)
       if ((e = cudaEventRecord(sl.copied, s->copyStream)) != cudaSuccess) { return cudaFail(e, "server: event"); }
       if ((e = cudaStreamWaitEvent(st, sl.copied, 0)) != cudaSuccess) { return cudaFail(e, "server: wait"); }
    }
+   if ((e = cudaEventRecord(sl.start, st)) != cudaSuccess) { return cudaFail(e, "server: event"); }
    // plan every request: word tasks, thermometer tasks, constant maps, single-field fallbacks
    std::vector<FieldTask> tasks[2];
    std::vector<BatchChunk> chunks[2];
@@ -292,6 +294,9 @@ static int issueLaunch(MKFServer *s, LaunchSlot &sl)
 // A launch finished: hand out the results, give the memory back (worker thread, under s->mu).
 static void completeLaunch(MKFServer *s, LaunchSlot &sl, int rc, const char *msg)
 {
+   float ms = 0.0f;
+   if (rc == MKF_OK && cudaEventElapsedTime(&ms, sl.start, sl.done) == cudaSuccess) { s->launchDeviceSec += 1e-3 * ms; }
+   cudaGetLastError();
    for (Request *r : sl.reqs) {
       if (r->staged) {
          s->arena.release(r->staged, r->fieldBytes);
@@ -387,8 +392,11 @@ static void workerLoop(MKFServer *s)
                s->fieldsLaunched += sl->reqs.size();
                s->maxInLaunch = std::max<uint32_t>(s->maxInLaunch, (uint32_t)sl->reqs.size());
                lk.unlock();
+               const Clock::time_point t0 = Clock::now();
                const int rc = issueLaunch(s, *sl);
+               const double dt = std::chrono::duration<double>(Clock::now() - t0).count();
                lk.lock();
+               s->planHostSec += dt;
                if (rc != MKF_OK) {
                   // nothing of a failed launch is trusted: wait for what was issued, then fail it
                   cudaStreamSynchronize(sl->stream);
@@ -428,7 +436,8 @@ MKF_API int mkfServerCreate(MKFServer **ps, const MKFServerConfig *cfg)
    for (LaunchSlot &sl : s->slots) {
       if (e == cudaSuccess) { e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking); }
       if (e == cudaSuccess) { e = cudaEventCreateWithFlags(&sl.copied, cudaEventDisableTiming); }
-      if (e == cudaSuccess) { e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming); }
+      if (e == cudaSuccess) { e = cudaEventCreate(&sl.start); }
+      if (e == cudaSuccess) { e = cudaEventCreate(&sl.done); }
       if (e == cudaSuccess) { e = cudaMalloc(&sl.counters, kServerCounters * sizeof(unsigned)); }
    }
    if (e != cudaSuccess) {
@@ -553,6 +562,8 @@ MKF_API int mkfServerStats(MKFServer *s, MKFServerStats *st, int reset)
    st->maxFieldsInLaunch = s->maxInLaunch;
    st->meanFieldsInLaunch = s->launches ? (double)s->fieldsLaunched / (double)s->launches : 0.0;
    st->deviceBytesInUse = s->arena.used();
+   st->launchDeviceSec = s->launchDeviceSec;
+   st->planHostSec = s->planHostSec;
    if (!v.empty()) {
       std::sort(v.begin(), v.end());
       auto q = [&](double p) { return v[std::min(v.size() - 1, (size_t)(p * (double)(v.size() - 1) + 0.5))]; };
@@ -566,6 +577,7 @@ MKF_API int mkfServerStats(MKFServer *s, MKFServerStats *st, int reset)
    if (reset) {
       s->latency.clear();
       s->failed = s->launches = s->fieldsLaunched = 0;
+      s->launchDeviceSec = s->planHostSec = 0.0;
       s->maxInLaunch = 0;
    }
    return MKF_OK;
@@ -586,6 +598,7 @@ MKF_API int mkfServerDestroy(MKFServer *s)
       if (sl.stream) { cudaStreamDestroy(sl.stream); }
       if (sl.copied) { cudaEventDestroy(sl.copied); }
       if (sl.done) { cudaEventDestroy(sl.done); }
+      if (sl.start) { cudaEventDestroy(sl.start); }
       if (sl.counters) { cudaFree(sl.counters); }
       sl.work.destroy();
       sl.results.destroy();
