@@ -109,6 +109,7 @@ int planBatchField(const MKFFieldDesc *pF, const MKFThreshSet *pT, int rowBase, 
 // Slab depth (planes of cells per work item) of a single-field launch of kernel family `family`
 // (tune.cu): the depth mkfTune measured best for this kind of field, else `def`.
 enum { kFamWords = 0, kFamThermo = 1, kFamThermoTma = 2 };
+static constexpr int kTmNumVariants = 4;  // variants of the TMA rank-table kernel (thermo_tma.cu)
 int tunedDepth(int family, int enc, int K, int X, int Y, int Z, int def);
 // Kernel variant (CTA shape, histogram copies) of such a launch: the one mkfTune measured best for
 // this kind of field, else `def`. Families without variants use 0.

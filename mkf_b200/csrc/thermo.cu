@@ -66,7 +66,6 @@ __device__ __forceinline__ unsigned long long warpItem(const P &a, long long it,
    const bool laneIn = x0 + lane >= xs && x0 + lane < xe;
    // bit j: row pair j of this lane is counted
    const uint32_t rowsOK = laneIn ? ((1u << jhi) - 1u) & ~((1u << jlo) - 1u) : 0u;
-   const uint32_t vx = laneIn ? 0xFFFFFFFFu : 0u;
    const long long rowStep = (long long)W * a.sy, planeStep = (long long)W * a.sz;
    const uint32_t rowBytes = (uint32_t)(rowStep * 4);
    const long long e00 = (long long)xl * a.sx + (long long)y0 * a.sy + (long long)z0 * a.sz;

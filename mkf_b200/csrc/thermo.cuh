@@ -327,8 +327,8 @@ __device__ __forceinline__ uint32_t cellCode(uint32_t R0, uint32_t R1, uint32_t 
 // and itemGrid), and its launch (MKF_ERR_UNSUPPORTED when it does not take it).
 static constexpr int kTmItemsPerSM = 80;  // four items per resident warp (20 per SM)
 bool thermoTmaEligible(const FusedArgs &a, int enc);
-// variant: CTA shape and histogram privatisation (kTmVariants in thermo_tma.cu), 0 = default.
-static constexpr int kTmNumVariants = 3;
+// variant: CTA shape, histogram privatisation and queue kind (kTmVariants in thermo_tma.cu,
+// kTmNumVariants of them), 0 = default.
 int launchThermoTma(const FusedArgs &a, int enc, int variant, cudaStream_t s);
 
 }  // namespace mkf

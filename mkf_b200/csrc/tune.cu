@@ -39,7 +39,7 @@ static int log2Class(int n)
    return b;
 }
 
-static constexpr int kVariantsOf[3] = {1, 1, 3};  // variants per family (words, rank table, TMA rank table)
+static constexpr int kVariantsOf[3] = {1, 1, kTmNumVariants};  // variants per family (words, rank table, TMA rank table)
 
 static std::mutex gTuneMu;
 static std::map<TuneKey, TuneVal> gTuned;

@@ -499,10 +499,11 @@ def test_tuning_keeps_counts(mkf, cuda):
     for (f, t), b in zip(cases, before):
         assert (u64(mkf.field_bpfd(f, t, 4)) == b).all()
     # the 16-threshold FP64 field takes the TMA-staged rank-table kernel: mkfTune recorded a depth
-    # and one of its variants, and every variant (CTA shape, histogram copies) keeps the counts
+    # and one of its variants, and every variant (CTA shape, histogram copies, queue kind) keeps
+    # the counts
     depth, variant = mkf.tuned(f64, cases[0][1], 4)
-    assert depth in (4, 8, 16, 32, 64, 128) and variant in (0, 1, 2)
-    for v in (0, 1, 2):
+    assert depth in (4, 8, 16, 32, 64, 128) and 0 <= variant < 4
+    for v in range(4):
         for dep in (8, 64):
             mkf.tune(f64, cases[0][1], 4, depth=dep, variant=v)
             assert mkf.tuned(f64, cases[0][1], 4) == (dep, v)
@@ -776,7 +777,7 @@ def test_benchmark_config_equals_reference_c_path(mkf, ref_oracle, cuda):
     want = np.stack([ref_oracle.bpfd_mt(host, (1024, 1024, Z), float(tv), mkf.BMC_GT, threads) for tv in t])
     assert (want.sum(axis=1) == 1023 * 1023 * (Z - 1)).all()
     del host
-    for depth, variant in ((None, 0), (128, 0), (64, 0), (32, 0), (8, 0), (4, 0), (128, 1), (64, 2)):
+    for depth, variant in ((None, 0), (128, 0), (64, 0), (32, 0), (8, 0), (4, 0), (128, 1), (64, 2), (128, 3), (32, 2)):
         if depth is not None:
             mkf.tune(f, t, mkf.BMC_GT, depth=depth, variant=variant)
         got = u64(mkf.field_bpfd(f, t, mkf.BMC_GT))
