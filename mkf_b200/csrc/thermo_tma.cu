@@ -58,7 +58,7 @@ static constexpr int kTmRows = 9;           // rows of a plane tile: 8 row pairs
 // one discard entry)
 static constexpr int kTmQueue = 32 + 8 * 31;  // drained after a plane once 32 are waiting
 // per-lane queue: entries per lane (a plane adds at most 8; drained after a plane once a lane
-// holds more than kTmLaneQ - 8), entry q of a lane at q * 32 + lane, discard entries at q = kTmLaneQ
+// holds more than kTmLaneQ - 8), entry q of a lane at q * 32 + lane
 static constexpr int kTmLaneQ = 12;
 static constexpr int kTmMaxK = 16;          // thresholds a 16-bit thermometer holds
 static constexpr int kTmMaxDepth = kThMaxDepth;  // planes per work item
@@ -76,7 +76,7 @@ struct TmaGeom
    static constexpr int BYTES = BX * kTmRows * (int)sizeof(T);   // bytes one TMA copy writes
    static constexpr int PITCH = (BYTES + 127) / 128 * 128;       // stage stride
    static constexpr bool LANEQ = kTmVariants[V].laneQueue != 0;
-   static constexpr int QWORDS = LANEQ ? (kTmLaneQ + 1) * 32 : kTmQueue + 1;  // queue entries per warp
+   static constexpr int QWORDS = LANEQ ? kTmLaneQ * 32 : kTmQueue + 1;  // queue entries per warp
 };
 
 // Set when a wait of this kernel ran out of polls (never in a correct run); read by mkfKernelFaults.
@@ -352,7 +352,10 @@ __global__ void __launch_bounds__(kTmVariants[V].warps * 32, 1)
 
    unsigned long long cells = 0;
    uint32_t masked = 0;  // masked cells counted (in smallest-rank row 16)
-   int qn = 0;           // wide cells queued (by the warp, or by this lane)
+   int qn = 0;           // wide cells queued by the warp (warp queue)
+   // per-lane queue: shared address of this lane's first entry and of its next one
+   const uint32_t qLane0 = (uint32_t)__cvta_generic_to_shared(queue) + (uint32_t)lane * 8u;
+   uint32_t qa = qLane0;
    for (long long it = first; it < a.nItems; it += nw) {
       const TmItem m = itemOf<G::ALIGN>(a, it, lane);
       cells += m.cells;
@@ -410,13 +413,21 @@ __global__ void __launch_bounds__(kTmVariants[V].warps * 32, 1)
             redSharedAt<0>(codeAddr((G0 | G1) & 0xFF000000u, rowAddr));
             redSharedAt<kHistRow * 4>(codeAddr(G1 & 0xFF000000u, rowAddr));
             redSharedAt<kHistRow * 8>(codeAddr((G0 & G1) & 0xFF000000u, rowAddr));
-            // cells crossing 4 or more thresholds join the warp's queue; every lane stores (the
-            // others into the discard entry), so the row body has no branch
-            const bool wide = pc < 13u;
+            // cells crossing 4 or more thresholds join the queue
             if (G::LANEQ) {
-               queue[32 * (wide ? qn : kTmLaneQ) + lane] = make_uint2(R0, R1);
-               qn += wide;
+               // two predicated stores and a predicated advance: no branch, no register pair
+               asm volatile(
+                   "{\n\t.reg .pred w;\n\t"
+                   "setp.lt.u32 w, %1, 13;\n\t"
+                   "@w st.shared.u32 [%0], %2;\n\t"
+                   "@w st.shared.u32 [%0+4], %3;\n\t"
+                   "@w add.u32 %0, %0, 256;\n\t}"
+                   : "+r"(qa)
+                   : "r"(pc), "r"(R0), "r"(R1)
+                   : "memory");
             } else {
+               // every lane stores (the others into the discard entry), so the row body has no branch
+               const bool wide = pc < 13u;
                const uint32_t wb = __ballot_sync(FULL, wide);
                queue[wide ? qn + __popc(wb & lanesBelow) : kTmQueue] = make_uint2(R0, R1);
                qn += __popc(wb);
@@ -427,9 +438,9 @@ __global__ void __launch_bounds__(kTmVariants[V].warps * 32, 1)
             Pprev = P;
          }
          if (G::LANEQ) {
-            if (__any_sync(FULL, qn > kTmLaneQ - 8)) {
-               drainLanes(queue, qn, hist32);
-               qn = 0;
+            if (__any_sync(FULL, qa > qLane0 + (kTmLaneQ - 8) * 256u)) {
+               drainLanes(queue, (int)((qa - qLane0) >> 8), hist32);
+               qa = qLane0;
             }
          } else if (qn >= 32) {
             drainWide(queue, qn, hist32);
@@ -440,7 +451,7 @@ __global__ void __launch_bounds__(kTmVariants[V].warps * 32, 1)
    }
    // the queue holds ranks only (no item coordinates): it is drained when full and once here
    if (G::LANEQ) {
-      if (__any_sync(FULL, qn > 0)) { drainLanes(queue, qn, hist32); }
+      if (__any_sync(FULL, qa != qLane0)) { drainLanes(queue, (int)((qa - qLane0) >> 8), hist32); }
    } else if (qn > 0) {
       drainWide(queue, qn, hist32);
    }
