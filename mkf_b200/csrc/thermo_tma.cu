@@ -415,12 +415,13 @@ __global__ void __launch_bounds__(kTmVariants[V].warps * 32, 1)
             redSharedAt<kHistRow * 8>(codeAddr((G0 & G1) & 0xFF000000u, rowAddr));
             // cells crossing 4 or more thresholds join the queue
             if (G::LANEQ) {
-               // two predicated stores and a predicated advance: no branch, no register pair
+               // a predicated 64-bit store and a predicated advance, no branch (measured against
+               // two 32-bit stores: 2 % faster; against skipping the stores when no lane of the
+               // warp has a wide cell: 3-4 % faster, even with 8 thresholds where none has)
                asm volatile(
                    "{\n\t.reg .pred w;\n\t"
                    "setp.lt.u32 w, %1, 13;\n\t"
-                   "@w st.shared.u32 [%0], %2;\n\t"
-                   "@w st.shared.u32 [%0+4], %3;\n\t"
+                   "@w st.shared.v2.u32 [%0], {%2, %3};\n\t"
                    "@w add.u32 %0, %0, 256;\n\t}"
                    : "+r"(qa)
                    : "r"(pc), "r"(R0), "r"(R1)
