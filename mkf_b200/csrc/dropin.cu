@@ -86,10 +86,14 @@ __global__ void __launch_bounds__(256) packMap(const __grid_constant__ PackArgs 
 }
 
 // One planar field whose rows are whole words (X a multiple of 32): map word i is elements
-// 32 i .. 32 i + 31 of the field, so the map is a flat pass with no row arithmetic. A warp takes 32
-// consecutive words per step: lane j loads element j of each (32 coalesced loads in flight), one
-// ballot per word, and lane i stores word i of the step (one coalesced 128-byte store).
-template <typename T>
+// 32 i .. 32 i + 31 of the field, so the map is a flat pass with no row arithmetic. A warp takes
+// kPackWords consecutive words per step: lane j loads element j of each (coalesced loads in
+// flight), one ballot per word, and lane i stores word i of the step. The grid is the resident
+// CTAs only, each warp looping over steps (measured on the 256^3 FP32 ball, events around the
+// call: 16 words per step on a resident grid 21.0-21.2 us, 32 words per step on 8 CTAs per SM
+// 23.0 us).
+static constexpr int kPackWords = 16;
+template <typename T, int U = kPackWords>
 __global__ void __launch_bounds__(256) packFlat(const __grid_constant__ PackArgs a)
 {
    const int lane = threadIdx.x & 31;
@@ -97,15 +101,15 @@ __global__ void __launch_bounds__(256) packFlat(const __grid_constant__ PackArgs
    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
    const T t = (T)a.t;
    const T *__restrict__ f0 = (const T *)a.f[0];
-   for (long long w0 = gw * 32; w0 < a.nWords; w0 += nw * 32) {
-      const int n = (int)min(32LL, a.nWords - w0);
+   for (long long w0 = gw * U; w0 < a.nWords; w0 += nw * U) {
+      const int n = (int)min((long long)U, a.nWords - w0);
       const T *p = f0 + w0 * 32 + lane;
-      T v[32];
+      T v[U];
 #pragma unroll
-      for (int u = 0; u < 32; u++) { v[u] = u < n ? __ldg(p + 32 * u) : T(0); }
+      for (int u = 0; u < U; u++) { v[u] = u < n ? __ldg(p + 32 * u) : T(0); }
       uint32_t mine = 0;
 #pragma unroll
-      for (int u = 0; u < 32; u++) {
+      for (int u = 0; u < U; u++) {
          const uint32_t word = __ballot_sync(FULL, (a.m >> relIdx(v[u], t)) & 1u);
          mine = (lane == u) ? word : mine;
       }
@@ -118,8 +122,9 @@ static void launchPack(const PackArgs &a, long long grid)
 {
    if (a.nF == 1 && a.sx == 1 && a.sy == a.X && a.sz == (int64_t)a.X * a.Y && (int64_t)a.rowWS * 32 == a.X &&
        (int64_t)a.planeWS == (int64_t)a.rowWS * a.Y) {
-      long long g = (a.nWords + 32 * 8 - 1) / (32 * 8);  // 8 warps of 32 words per CTA
-      const long long cap = (long long)smCount() * 8;
+      long long g = (a.nWords + kPackWords * 8 - 1) / (kPackWords * 8);  // 8 warps of kPackWords words per CTA
+      static std::atomic<int> occ{0};
+      const long long cap = (long long)smCount() * cachedOccupancy(occ, packFlat<T>, 256, 0);
       if (g > cap) { g = cap; }
       packFlat<T><<<(unsigned)(g < 1 ? 1 : g), 256>>>(a);
       return;
