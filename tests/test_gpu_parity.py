@@ -835,6 +835,28 @@ def test_tma_rank_table_kernel_against_oracle(mkf, oracle, cuda, dtype):
 
 
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_tma_rank_table_kernel_saturated_queue_every_variant(mkf, oracle, cuda, dtype):
+    """White noise under 16 thresholds spread over its range: nearly every cell crosses four or
+    more thresholds, so every lane queues a wide cell in every row pair and the queues fill to
+    their limit before each drain (per-lane queue: a drain after every plane; warp queue: several
+    per plane). Every kernel variant, two slab depths, against the oracle; no wait ran out."""
+    rng = np.random.default_rng(4242)
+    shape = (40, 26, 96)
+    f = rng.standard_normal(shape).astype(dtype)
+    Z, Y, X = shape
+    fd = to_dev(f, cuda)
+    t = np.linspace(-1.6, 1.6, 16)
+    want = oracle.bpfd_field(f, (X, Y, Z), t, mkf.BMC_GT)
+    mkf.lib().mkfKernelFaults(1)
+    for variant in range(4):
+        for depth in (8, 32):
+            mkf.tune(fd, t, mkf.BMC_GT, depth=depth, variant=variant)
+            assert (u64(mkf.field_bpfd(fd, t, mkf.BMC_GT)) == want).all(), (variant, depth)
+    mkf.tune(fd, t, mkf.BMC_GT, depth=0)
+    assert mkf.lib().mkfKernelFaults(1) == 0
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
 def test_tma_rank_table_kernel_exact_path_and_depths(mkf, oracle, cuda, dtype):
     """The TMA-staged kernel's exact path: elements equal to thresholds (ties of the whole value,
     and for FP64 of the high word only), infinities, NaNs and huge magnitudes, under every relation;
