@@ -337,7 +337,11 @@ void floatBoundsPlain(double t, double &tlo, double &thi) { floatBounds(t, tlo, 
 // Split one field of a batch: constant maps go to `consts` (rows offset by rowBase). One or two
 // other thresholds fill `w` for the batched word kernel (returns kPlanWords); more thresholds that
 // share one thermometer relation and fit the rank table fill `t` for the batched thermometer
-// kernel (kPlanThermo); otherwise the field takes the single-field path (kPlanSingle).
+// kernel (kPlanThermo), unless the field has kSoloVoxels or more: such a field fills the GPU on
+// its own, and the single-field kernels (the word kernel for a few thresholds, the TMA-staged rank
+// table on aligned rows) count it faster than the batched rank-table kernel. Those fields, and
+// the rest, take the single-field path (kPlanSingle).
+static constexpr double kSoloVoxels = (double)(1 << 23);
 int planBatchField(const MKFFieldDesc *pF, const MKFThreshSet *pT, int rowBase, FieldTask &t, WordTask &w,
                    std::vector<ConstEntry> &consts, bool &anyVarying, int depth)
 {
@@ -389,7 +393,7 @@ int planBatchField(const MKFFieldDesc *pF, const MKFThreshSet *pT, int rowBase, 
       prepareWordTask(w, pF->enc, depth);
       return kPlanWords;
    }
-   if (cls0 < 0) { return kPlanSingle; }
+   if (cls0 < 0 || (double)X * (double)Y * (double)Z >= kSoloVoxels) { return kPlanSingle; }
    std::stable_sort(idx, idx + n, [&](int x, int y) { return pT->t[x] < pT->t[y]; });
    t.f = pF->p;
    t.sx = planar ? 1 : pF->stride[0];

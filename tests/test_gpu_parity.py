@@ -553,6 +553,34 @@ def test_batch_fields_with_three_to_six_thresholds(mkf, oracle, cuda):
     plan.close()
 
 
+def test_batch_plan_with_fields_that_fill_the_gpu(mkf, cuda):
+    """Fields of 2^23 voxels or more with 3+ thresholds of one relation leave the batched
+    rank-table kernel for the single-field kernels inside the same plan (word kernel for a few
+    thresholds, the TMA rank table on aligned rows, the global-load one on unaligned rows), with
+    their constant-map thresholds; small fields stay batched. Plan launch, graph replay and the
+    one-shot batch call equal the single-field counts."""
+    import torch
+
+    g = torch.Generator(device=cuda).manual_seed(91)
+    big = [torch.randn((128, 256, 256), dtype=torch.float64, device=cuda, generator=g),
+           torch.randn((132, 250, 258), dtype=torch.float32, device=cuda, generator=g),
+           torch.randn((140, 240, 255), dtype=torch.float32, device=cuda, generator=g),  # rows off 16 B
+           torch.randn((128, 256, 256), dtype=torch.float32, device=cuda, generator=g)]
+    small = [torch.randn((30, 40, 50), dtype=torch.float64, device=cuda, generator=g),
+             torch.randn((20, 33, 64), dtype=torch.float32, device=cuda, generator=g)]
+    fields = big + small
+    ths = [list(np.linspace(-1.5, 1.5, 16)), list(np.linspace(-1, 1, 8)) + [float("nan")],
+           list(np.linspace(-1.2, 1.2, 12)), [-0.5, 0.0, 0.5],
+           list(np.linspace(-1, 1, 9)), [-0.3, 0.1, 0.4, 0.8]]
+    masks = [mkf.BMC_GT, mkf.BMC_LT | mkf.BMC_EQ, mkf.BMC_GT | mkf.BMC_EQ, mkf.BMC_LT, mkf.BMC_GT, mkf.BMC_LT]
+    want = np.concatenate([u64(mkf.field_bpfd(f, t, m)) for f, t, m in zip(fields, ths, masks)])
+    plan = mkf.BatchPlan(fields, ths, masks)
+    assert (u64(plan.launch()) == want).all()
+    assert (u64(plan.launch_graph()) == want).all()
+    plan.close()
+    assert (u64(mkf.batch_bpfd(fields, ths, masks)) == want).all()
+
+
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 def test_rank_table_kernel_on_all_ones_regions(mkf, oracle, cuda, dtype):
     """Large regions above every threshold: work items of 64 (default) and 128 (tuned) planes
