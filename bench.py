@@ -52,11 +52,12 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true", help="skip the batched, serving and in-situ workloads (and the reference CUDA point of the reference arm)")
-    ap.add_argument("--profile", choices=["field", "batch", "planewave"], default=None,
+    ap.add_argument("--profile", choices=["field", "batch", "planewave", "dropin"], default=None,
                     help="run one small case for a profiler instead of the benchmark: 'field' = one "
                          "GRF (--side, --dtype, --thresholds), 'batch' = the uneven ball batch (--fields), "
                          "'planewave' = one 1024 x 1024 x --side FP32 step of the in-situ series, "
-                         "thresholds {-0.5, 0, 0.5}")
+                         "thresholds {-0.5, 0, 0.5}, 'dropin' = the drop-in pair binMapCUDA + "
+                         "mkfCUDAGetBPFD on the 256^3 FP32 ball, threshold 0")
     ap.add_argument("--side", type=int, default=512)
     ap.add_argument("--dtype", choices=["f32", "f64"], default="f64")
     ap.add_argument("--thresholds", default="16", help="a count n (linspace(-2, 2, n)) or a comma list of values")
@@ -1004,6 +1005,16 @@ def run_profile_case(args):
             mkf_b200.field_bpfd(f, t, mkf_b200.BMC_GT, out=out)
 
         vox, nbytes, what = f.numel(), f.numel() * 4, f"1024 x 1024 x {args.side} FP32 plane waves, 3 thresholds"
+    elif args.profile == "dropin":
+        f = ball256_torch(dev)
+        pbm0, org0, _ = mkf_b200.bin_map_cuda(f, ">", 0.0)
+        counts = torch.zeros(256, dtype=torch.int64, device=dev)
+
+        def launch():
+            pbm, org, _ = mkf_b200.bin_map_cuda(f, ">", 0.0, out=pbm0)
+            mkf_b200.get_bpfd(pbm, org, out=counts)
+
+        vox, nbytes, what = f.numel(), f.numel() * 4, "256^3 FP32 ball, threshold 0, drop-in pair"
     else:
         fields = ball_fields(args.fields, 77, dev)
         plan = mkf_b200.BatchPlan(fields, [[0.0]] * len(fields))  # tunes the slab depth at creation
