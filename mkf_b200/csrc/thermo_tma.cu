@@ -348,7 +348,9 @@ __global__ void __launch_bounds__(kTmVariants[V].warps * 32, 1)
       ++g;
       return true;
    };
-   // thermometer of a rank and its complement: T | ~T << 16, T = bits [0, r)
+   // thermometer of a rank and its complement: T | ~T << 16, T = bits [0, r); the x neighbour's
+   // is formed here from its shuffled rank (one shuffle per row, not two: shuffles share the pipe
+   // of the tile loads and the histogram atomics; measured 1 % faster)
    auto thermoV = [](uint32_t r) { return thermo(r) * 0xFFFF0001u + 0xFFFF0000u; };
 
    unsigned long long cells = 0;
@@ -366,13 +368,13 @@ __global__ void __launch_bounds__(kTmVariants[V].warps * 32, 1)
          uint32_t r[kTmRows];
          if (!plane(m.xoff, r)) { fault = true; break; }
          uint32_t rR = __shfl_down_sync(FULL, r[0], 1);
-         uint32_t Vt = thermoV(r[0]), VR = __shfl_down_sync(FULL, Vt, 1);
+         uint32_t Vt = thermoV(r[0]), VR = thermoV(rR);
          uint32_t ePrev = rR * 256u + r[0], Pprev = Vt & VR;
 #pragma unroll
          for (int j = 0; j < 8; ++j) {
             rR = __shfl_down_sync(FULL, r[j + 1], 1);
             Vt = thermoV(r[j + 1]);
-            VR = __shfl_down_sync(FULL, Vt, 1);
+            VR = thermoV(rR);
             const uint32_t e = rR * 256u + r[j + 1], P = Vt & VR;
             sF[j] = e * 65536u + ePrev;
             sV[j] = P & Pprev;
@@ -384,14 +386,14 @@ __global__ void __launch_bounds__(kTmVariants[V].warps * 32, 1)
          uint32_t r[kTmRows];
          if (!plane(m.xoff, r)) { fault = true; break; }
          uint32_t rR = __shfl_down_sync(FULL, r[0], 1);
-         uint32_t Vt = thermoV(r[0]), VR = __shfl_down_sync(FULL, Vt, 1);
+         uint32_t Vt = thermoV(r[0]), VR = thermoV(rR);
          uint32_t ePrev = rR * 256u + r[0];
          uint32_t Pprev = Vt & VR;
 #pragma unroll
          for (int j = 0; j < 8; ++j) {
             rR = __shfl_down_sync(FULL, r[j + 1], 1);
             Vt = thermoV(r[j + 1]);
-            VR = __shfl_down_sync(FULL, Vt, 1);
+            VR = thermoV(rR);
             const uint32_t e = rR * 256u + r[j + 1];
             const uint32_t P = Vt & VR;
             const uint32_t fc = e * 65536u + ePrev;  // face ranks: (x,y) (x+1,y) (x,y+1) (x+1,y+1)
